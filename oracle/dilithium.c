@@ -1,0 +1,783 @@
+/*
+ * CPU oracle: CRYSTALS-Dilithium round 3 (v3.1), parameter sets 2/3/5 chosen at run time.
+ *
+ * TEST INFRASTRUCTURE ONLY -- the checker for the CUDA product and the timed CPU baseline.
+ * Nothing in cudilithium_b200 links or calls this file.
+ *
+ * Each routine restates what the reference computes on the GPU (file:line in the
+ * reference tree):
+ *   parameters ............ include/params.h:7-73
+ *   montgomery / reduce ... include/ntt.cuh:64-72, include/reduce.cuh:42-78
+ *   rounding .............. include/rounding.cuh:22-107
+ *   chknorm ............... include/poly.cuh:31-54
+ *   NTT / invNTT .......... src/ntt.cu:24-207 (zetas, CT/GS butterflies, f = 41978)
+ *   keypair ............... src/keypair.cu:35-311 (seed derivation :53-67, ExpandS nonces
+ *                           l and L+k :84-87/:202-205, ExpandA nonce :143-147, packing)
+ *   sign .................. src/api.cu:63-452 (mu, rho' :137-152; smallest accepted nonce
+ *                           :388-411), src/sign.cu (ExpandMask kappa = L*nonce+l :488-499,
+ *                           w1 packing :668-682, SampleInBall :767-787, rejection order and
+ *                           MakeHint :1026-1144, z packing :1152-1192)
+ *   verify ................ src/verify.cu:35-322, src/api.cu:454-515
+ * Where the reference's GPU samplers stop at a fixed buffer (ExpandA after 5 SHAKE128
+ * blocks, SampleInBall after one SHAKE256 block, ExpandS after 2/3 blocks) this file keeps
+ * squeezing the same stream, as benches/bench_rej_sampling.cu:571-593 does on the CPU; the
+ * two agree whenever the reference's result is defined (the short buffers run out only with
+ * negligible probability).
+ *
+ * Pinning: ora_tvecs() regenerates the reference's test-vector file
+ * (tests/test_vectors.cu:40-217) and its sha256 must equal the digests in
+ * tests/CMakeLists.txt:21-23 for all three parameter sets.
+ */
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "oracle.h"
+
+#define N ORA_N
+#define Q ORA_Q
+#define D 13
+#define QINV 58728449 /* q^-1 mod 2^32 */
+#define MAXK 8
+#define MAXL 7
+
+/* ---------------------------------------------------------------- parameters */
+
+int ora_params_get(int mode, ora_params *p) {
+    memset(p, 0, sizeof *p);
+    p->mode = mode;
+    switch (mode) {
+        case 2:
+            p->k = 4; p->l = 4; p->eta = 2; p->tau = 39; p->beta = 78;
+            p->gamma1 = 1 << 17; p->gamma2 = (Q - 1) / 88; p->omega = 80;
+            break;
+        case 3:
+            p->k = 6; p->l = 5; p->eta = 4; p->tau = 49; p->beta = 196;
+            p->gamma1 = 1 << 19; p->gamma2 = (Q - 1) / 32; p->omega = 55;
+            break;
+        case 5:
+            p->k = 8; p->l = 7; p->eta = 2; p->tau = 60; p->beta = 120;
+            p->gamma1 = 1 << 19; p->gamma2 = (Q - 1) / 32; p->omega = 75;
+            break;
+        default:
+            return -1;
+    }
+    p->polyz_packed = (p->gamma1 == (1 << 17)) ? 576 : 640;
+    p->polyw1_packed = (p->gamma2 == (Q - 1) / 88) ? 192 : 128;
+    p->polyeta_packed = (p->eta == 2) ? 96 : 128;
+    p->pk_bytes = ORA_SEEDBYTES + p->k * 320;
+    p->sk_bytes = 3 * ORA_SEEDBYTES + (p->l + p->k) * p->polyeta_packed + p->k * 416;
+    p->sig_bytes = ORA_SEEDBYTES + p->l * p->polyz_packed + p->omega + p->k;
+    return 0;
+}
+
+/* ---------------------------------------------------------------- arithmetic */
+
+int32_t ora_montgomery_reduce(int64_t a) {
+    int32_t t = (int32_t)((uint32_t)(uint64_t)a * (uint32_t)QINV);
+    return (int32_t)((a - (int64_t)t * Q) >> 32);
+}
+
+static int32_t reduce32(int32_t a) {
+    int32_t t = (a + (1 << 22)) >> 23;
+    return a - t * Q;
+}
+
+static int32_t caddq(int32_t a) { return a + ((a >> 31) & Q); }
+
+static int32_t power2round(int32_t *a0, int32_t a) {
+    int32_t a1 = (a + (1 << (D - 1)) - 1) >> D;
+    *a0 = a - (a1 << D);
+    return a1;
+}
+
+static int32_t decompose(const ora_params *p, int32_t *a0, int32_t a) {
+    int32_t a1 = (a + 127) >> 7;
+    if (p->gamma2 == (Q - 1) / 32) {
+        a1 = (a1 * 1025 + (1 << 21)) >> 22;
+        a1 &= 15;
+    } else {
+        a1 = (a1 * 11275 + (1 << 23)) >> 24;
+        a1 ^= ((43 - a1) >> 31) & a1;
+    }
+    *a0 = a - a1 * 2 * p->gamma2;
+    *a0 -= (((Q - 1) / 2 - *a0) >> 31) & Q;
+    return a1;
+}
+
+static int make_hint(const ora_params *p, int32_t a0, int32_t a1) {
+    return (a0 > p->gamma2 || a0 < -p->gamma2 || (a0 == -p->gamma2 && a1 != 0)) ? 1 : 0;
+}
+
+static int32_t use_hint(const ora_params *p, int32_t a, int hint) {
+    int32_t a0, a1 = decompose(p, &a0, a);
+    if (!hint) return a1;
+    if (p->gamma2 == (Q - 1) / 32) return (a0 > 0) ? ((a1 + 1) & 15) : ((a1 - 1) & 15);
+    if (a0 > 0) return (a1 == 43) ? 0 : a1 + 1;
+    return (a1 == 0) ? 43 : a1 - 1;
+}
+
+/* 1 if some coefficient has |a| >= bound (include/poly.cuh:31-54). */
+static int chknorm(const int32_t *a, int32_t bound) {
+    int i;
+    if (bound > (Q - 1) / 8) return 1;
+    for (i = 0; i < N; i++) {
+        int32_t t = a[i] >> 31;
+        t = a[i] - (t & 2 * a[i]);
+        if (t >= bound) return 1;
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------- NTT */
+
+static int32_t g_zetas[N];
+static int g_zetas_ready = 0;
+
+static unsigned brv8(unsigned x) {
+    unsigned r = 0, i;
+    for (i = 0; i < 8; i++) r |= ((x >> i) & 1u) << (7 - i);
+    return r;
+}
+
+/* zetas[i] = 2^32 * 1753^brv8(i) mod q, centred; zetas[0] is unused and kept 0 as in
+ * src/ntt.cu:24. */
+static void zetas_init(void) {
+    int i;
+    uint64_t mont = (1ULL << 32) % Q;
+    if (g_zetas_ready) return;
+    for (i = 0; i < N; i++) {
+        uint64_t e = brv8((unsigned)i), r = 1, b = 1753;
+        while (e) {
+            if (e & 1) r = r * b % Q;
+            b = b * b % Q;
+            e >>= 1;
+        }
+        r = r * mont % Q;
+        g_zetas[i] = (int32_t)(r > (Q - 1) / 2 ? (int64_t)r - Q : (int64_t)r);
+    }
+    g_zetas[0] = 0;
+    g_zetas_ready = 1;
+}
+
+void ora_ntt(int32_t a[N]) {
+    unsigned len, start, j, k = 0;
+    zetas_init();
+    for (len = 128; len > 0; len >>= 1) {
+        for (start = 0; start < N; start = j + len) {
+            int32_t zeta = g_zetas[++k];
+            for (j = start; j < start + len; ++j) {
+                int32_t t = ora_montgomery_reduce((int64_t)zeta * a[j + len]);
+                a[j + len] = a[j] - t;
+                a[j] = a[j] + t;
+            }
+        }
+    }
+}
+
+void ora_invntt_tomont(int32_t a[N]) {
+    unsigned start, len, j, k = 256;
+    const int32_t f = 41978; /* mont^2 / 256 */
+    zetas_init();
+    for (len = 1; len < N; len <<= 1) {
+        for (start = 0; start < N; start = j + len) {
+            int32_t zeta = -g_zetas[--k];
+            for (j = start; j < start + len; ++j) {
+                int32_t t = a[j];
+                a[j] = t + a[j + len];
+                a[j + len] = t - a[j + len];
+                a[j + len] = ora_montgomery_reduce((int64_t)zeta * a[j + len]);
+            }
+        }
+    }
+    for (j = 0; j < N; ++j) a[j] = ora_montgomery_reduce((int64_t)f * a[j]);
+}
+
+static void pointwise(int32_t *c, const int32_t *a, const int32_t *b) {
+    int i;
+    for (i = 0; i < N; i++) c[i] = ora_montgomery_reduce((int64_t)a[i] * b[i]);
+}
+
+void ora_ntt_mul_batch(int32_t *a, const int32_t *b, size_t n, int nthreads) {
+    long i;
+    zetas_init();
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+#endif
+    for (i = 0; i < (long)n; i++) {
+        int32_t *ai = a + (size_t)i * N;
+        ora_ntt(ai);
+        pointwise(ai, ai, b + (size_t)i * N);
+        ora_invntt_tomont(ai);
+    }
+    (void)nthreads;
+}
+
+/* ---------------------------------------------------------------- bit packing */
+
+/* Little-endian bit stream of n values of `bits` bits each; every Dilithium packing
+ * (t1 10b, t0 13b, eta 3b/4b, z 18b/20b, w1 6b/4b) is this layout. */
+static void pack_bits(uint8_t *out, const uint32_t *v, int n, int bits) {
+    int i;
+    uint64_t acc = 0;
+    int nacc = 0, o = 0;
+    for (i = 0; i < n; i++) {
+        acc |= (uint64_t)(v[i] & ((1u << bits) - 1)) << nacc;
+        nacc += bits;
+        while (nacc >= 8) {
+            out[o++] = (uint8_t)acc;
+            acc >>= 8;
+            nacc -= 8;
+        }
+    }
+    if (nacc) out[o++] = (uint8_t)acc;
+}
+
+static void unpack_bits(uint32_t *v, const uint8_t *in, int n, int bits) {
+    int i, pos = 0;
+    uint64_t acc = 0;
+    int nacc = 0;
+    for (i = 0; i < n; i++) {
+        while (nacc < bits) {
+            acc |= (uint64_t)in[pos++] << nacc;
+            nacc += 8;
+        }
+        v[i] = (uint32_t)(acc & ((1u << bits) - 1));
+        acc >>= bits;
+        nacc -= bits;
+    }
+}
+
+static void pack_offset(uint8_t *out, const int32_t *a, int32_t off, int bits) {
+    uint32_t v[N];
+    int i;
+    for (i = 0; i < N; i++) v[i] = (uint32_t)(off - a[i]);
+    pack_bits(out, v, N, bits);
+}
+
+static void unpack_offset(int32_t *a, const uint8_t *in, int32_t off, int bits) {
+    uint32_t v[N];
+    int i;
+    unpack_bits(v, in, N, bits);
+    for (i = 0; i < N; i++) a[i] = off - (int32_t)v[i];
+}
+
+static int eta_bits(const ora_params *p) { return p->eta == 2 ? 3 : 4; }
+static int z_bits(const ora_params *p) { return p->gamma1 == (1 << 17) ? 18 : 20; }
+static int w1_bits(const ora_params *p) { return p->gamma2 == (Q - 1) / 88 ? 6 : 4; }
+
+static void pack_w1(const ora_params *p, uint8_t *out, const int32_t *w1) {
+    uint32_t v[N];
+    int i;
+    for (i = 0; i < N; i++) v[i] = (uint32_t)w1[i];
+    pack_bits(out, v, N, w1_bits(p));
+}
+
+/* ---------------------------------------------------------------- samplers */
+
+/* ExpandA entry (i,j): SHAKE128(rho || j || i), 23-bit candidates < q. */
+static void poly_uniform(int32_t *a, const uint8_t rho[32], uint16_t nonce) {
+    uint8_t in[34], buf[3];
+    ora_xof st;
+    int ctr = 0;
+    memcpy(in, rho, 32);
+    in[32] = (uint8_t)nonce;
+    in[33] = (uint8_t)(nonce >> 8);
+    ora_xof_init(&st, ORA_SHAKE128_RATE);
+    ora_xof_absorb(&st, in, 34);
+    ora_xof_finalize(&st);
+    while (ctr < N) {
+        uint32_t t;
+        ora_xof_squeeze(&st, buf, 3);
+        t = (uint32_t)buf[0] | ((uint32_t)buf[1] << 8) | ((uint32_t)(buf[2] & 0x7F) << 16);
+        if (t < (uint32_t)Q) a[ctr++] = (int32_t)t;
+    }
+}
+
+void ora_expand_a(int mode, int32_t *mat, const uint8_t rho[32]) {
+    ora_params p;
+    int i, j;
+    ora_params_get(mode, &p);
+    for (i = 0; i < p.k; i++)
+        for (j = 0; j < p.l; j++) poly_uniform(mat + (size_t)(i * p.l + j) * N, rho, (uint16_t)((i << 8) + j));
+}
+
+/* ExpandS entry: SHAKE256(rho' || nonce), nibbles rejected at 15 (eta 2) or 9 (eta 4). */
+static void poly_uniform_eta(const ora_params *p, int32_t *a, const uint8_t rhoprime[64], uint16_t nonce) {
+    uint8_t in[66], b;
+    ora_xof st;
+    int ctr = 0;
+    memcpy(in, rhoprime, 64);
+    in[64] = (uint8_t)nonce;
+    in[65] = (uint8_t)(nonce >> 8);
+    ora_xof_init(&st, ORA_SHAKE256_RATE);
+    ora_xof_absorb(&st, in, 66);
+    ora_xof_finalize(&st);
+    while (ctr < N) {
+        uint32_t t0, t1;
+        ora_xof_squeeze(&st, &b, 1);
+        t0 = b & 0x0F;
+        t1 = b >> 4;
+        if (p->eta == 2) {
+            if (t0 < 15) a[ctr++] = 2 - (int32_t)(t0 - (205 * t0 >> 10) * 5);
+            if (t1 < 15 && ctr < N) a[ctr++] = 2 - (int32_t)(t1 - (205 * t1 >> 10) * 5);
+        } else {
+            if (t0 < 9) a[ctr++] = 4 - (int32_t)t0;
+            if (t1 < 9 && ctr < N) a[ctr++] = 4 - (int32_t)t1;
+        }
+    }
+}
+
+/* ExpandMask entry: SHAKE256(rho' || kappa), 5 blocks, gamma1 - (18/20-bit values). */
+static void poly_uniform_gamma1(const ora_params *p, int32_t *a, const uint8_t rhoprime[64], uint16_t nonce) {
+    uint8_t in[66], buf[5 * ORA_SHAKE256_RATE];
+    memcpy(in, rhoprime, 64);
+    in[64] = (uint8_t)nonce;
+    in[65] = (uint8_t)(nonce >> 8);
+    ora_shake256(buf, sizeof buf, in, 66);
+    unpack_offset(a, buf, p->gamma1, z_bits(p));
+}
+
+void ora_expand_mask(int mode, int32_t *y, const uint8_t rhoprime[64], uint16_t nonce) {
+    ora_params p;
+    int j;
+    ora_params_get(mode, &p);
+    for (j = 0; j < p.l; j++)
+        poly_uniform_gamma1(&p, y + (size_t)j * N, rhoprime, (uint16_t)(p.l * nonce + j));
+}
+
+/* SampleInBall (src/sign.cu:767-787, src/verify.cu:222-244). */
+void ora_challenge(int mode, int32_t c[N], const uint8_t seed[32]) {
+    ora_params p;
+    ora_xof st;
+    uint8_t buf[8], b;
+    uint64_t signs = 0;
+    int i;
+    ora_params_get(mode, &p);
+    ora_xof_init(&st, ORA_SHAKE256_RATE);
+    ora_xof_absorb(&st, seed, 32);
+    ora_xof_finalize(&st);
+    ora_xof_squeeze(&st, buf, 8);
+    for (i = 0; i < 8; i++) signs |= (uint64_t)buf[i] << (8 * i);
+    memset(c, 0, sizeof(int32_t) * N);
+    for (i = N - p.tau; i < N; i++) {
+        do {
+            ora_xof_squeeze(&st, &b, 1);
+        } while (b > i);
+        c[i] = c[b];
+        c[b] = 1 - 2 * (int32_t)(signs & 1);
+        signs >>= 1;
+    }
+}
+
+/* ---------------------------------------------------------------- keypair */
+
+void ora_seed_from_ctr(uint8_t seed[32], uint64_t ctr) {
+    uint8_t b[8];
+    int i;
+    for (i = 0; i < 8; i++) b[i] = (uint8_t)(ctr >> (8 * i));
+    ora_shake128(seed, 32, b, 8);
+}
+
+int ora_keypair_from_seed(int mode, uint8_t *pk, uint8_t *sk, const uint8_t seed[32]) {
+    ora_params p;
+    uint8_t seedbuf[128];
+    const uint8_t *rho, *rhoprime, *key;
+    static __thread int32_t mat[MAXK * MAXL * N];
+    int32_t s1[MAXL][N], s1hat[MAXL][N], s2[MAXK][N], t[MAXK][N], t1[MAXK][N], t0[MAXK][N];
+    uint8_t tr[32];
+    int i, j, c;
+    if (ora_params_get(mode, &p)) return -1;
+    ora_shake256(seedbuf, 128, seed, 32);
+    rho = seedbuf;
+    rhoprime = seedbuf + 32;
+    key = seedbuf + 96;
+    ora_expand_a(mode, mat, rho);
+    for (j = 0; j < p.l; j++) poly_uniform_eta(&p, s1[j], rhoprime, (uint16_t)j);
+    for (i = 0; i < p.k; i++) poly_uniform_eta(&p, s2[i], rhoprime, (uint16_t)(p.l + i));
+    for (j = 0; j < p.l; j++) {
+        memcpy(s1hat[j], s1[j], sizeof s1hat[j]);
+        ora_ntt(s1hat[j]);
+    }
+    for (i = 0; i < p.k; i++) {
+        int32_t tmp[N];
+        memset(t[i], 0, sizeof t[i]);
+        for (j = 0; j < p.l; j++) {
+            pointwise(tmp, mat + (size_t)(i * p.l + j) * N, s1hat[j]);
+            for (c = 0; c < N; c++) t[i][c] += tmp[c];
+        }
+        for (c = 0; c < N; c++) t[i][c] = reduce32(t[i][c]);
+        ora_invntt_tomont(t[i]);
+        for (c = 0; c < N; c++) {
+            int32_t v = caddq(t[i][c] + s2[i][c]);
+            t1[i][c] = power2round(&t0[i][c], v);
+        }
+    }
+    /* pk = rho || t1 */
+    memcpy(pk, rho, 32);
+    for (i = 0; i < p.k; i++) {
+        uint32_t v[N];
+        for (c = 0; c < N; c++) v[c] = (uint32_t)t1[i][c];
+        pack_bits(pk + 32 + i * 320, v, N, 10);
+    }
+    ora_shake256(tr, 32, pk, (size_t)p.pk_bytes);
+    /* sk = rho || key || tr || s1 || s2 || t0 */
+    memcpy(sk, rho, 32);
+    memcpy(sk + 32, key, 32);
+    memcpy(sk + 64, tr, 32);
+    {
+        uint8_t *o = sk + 96;
+        for (j = 0; j < p.l; j++, o += p.polyeta_packed) pack_offset(o, s1[j], p.eta, eta_bits(&p));
+        for (i = 0; i < p.k; i++, o += p.polyeta_packed) pack_offset(o, s2[i], p.eta, eta_bits(&p));
+        for (i = 0; i < p.k; i++, o += 416) pack_offset(o, t0[i], 1 << (D - 1), 13);
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------- sign */
+
+int ora_sign_rhoprime(int mode, uint8_t *sig, const uint8_t *m, size_t mlen, const uint8_t *sk,
+                      const uint8_t *rhoprime_in, int *attempts) {
+    ora_params p;
+    static __thread int32_t mat[MAXK * MAXL * N];
+    int32_t s1[MAXL][N], s2[MAXK][N], t0[MAXK][N];
+    int32_t y[MAXL][N], z[MAXL][N], w1[MAXK][N], w0[MAXK][N], h[MAXK][N], cp[N];
+    uint8_t mu[64], rhoprime[64], keymu[96], w1packed[MAXK * 192], ctilde[32];
+    const uint8_t *rho = sk, *key = sk + 32, *tr = sk + 64;
+    uint32_t nonce = 0;
+    int i, j, c, att = 0;
+    ora_xof st;
+    if (ora_params_get(mode, &p)) return -1;
+    {
+        const uint8_t *o = sk + 96;
+        for (j = 0; j < p.l; j++, o += p.polyeta_packed) unpack_offset(s1[j], o, p.eta, eta_bits(&p));
+        for (i = 0; i < p.k; i++, o += p.polyeta_packed) unpack_offset(s2[i], o, p.eta, eta_bits(&p));
+        for (i = 0; i < p.k; i++, o += 416) unpack_offset(t0[i], o, 1 << (D - 1), 13);
+    }
+    /* mu = SHAKE256(tr || m, 64) */
+    ora_xof_init(&st, ORA_SHAKE256_RATE);
+    ora_xof_absorb(&st, tr, 32);
+    ora_xof_absorb(&st, m, mlen);
+    ora_xof_finalize(&st);
+    ora_xof_squeeze(&st, mu, 64);
+    if (rhoprime_in) {
+        memcpy(rhoprime, rhoprime_in, 64);
+    } else {
+        /* rho' = SHAKE256(key || mu, 64) */
+        memcpy(keymu, key, 32);
+        memcpy(keymu + 32, mu, 64);
+        ora_shake256(rhoprime, 64, keymu, 96);
+    }
+    ora_expand_a(mode, mat, rho);
+    for (j = 0; j < p.l; j++) ora_ntt(s1[j]);
+    for (i = 0; i < p.k; i++) {
+        ora_ntt(s2[i]);
+        ora_ntt(t0[i]);
+    }
+    for (;;) {
+        int rej = 0, nh = 0;
+        if (att >= 65536) return -2;
+        att++;
+        for (j = 0; j < p.l; j++) poly_uniform_gamma1(&p, y[j], rhoprime, (uint16_t)(p.l * nonce + j));
+        nonce++;
+        for (j = 0; j < p.l; j++) {
+            memcpy(z[j], y[j], sizeof z[j]);
+            ora_ntt(z[j]);
+        }
+        for (i = 0; i < p.k; i++) {
+            int32_t tmp[N];
+            memset(w1[i], 0, sizeof w1[i]);
+            for (j = 0; j < p.l; j++) {
+                pointwise(tmp, mat + (size_t)(i * p.l + j) * N, z[j]);
+                for (c = 0; c < N; c++) w1[i][c] += tmp[c];
+            }
+            for (c = 0; c < N; c++) w1[i][c] = reduce32(w1[i][c]);
+            ora_invntt_tomont(w1[i]);
+            for (c = 0; c < N; c++) w1[i][c] = decompose(&p, &w0[i][c], caddq(w1[i][c]));
+            pack_w1(&p, w1packed + i * p.polyw1_packed, w1[i]);
+        }
+        ora_xof_init(&st, ORA_SHAKE256_RATE);
+        ora_xof_absorb(&st, mu, 64);
+        ora_xof_absorb(&st, w1packed, (size_t)p.k * p.polyw1_packed);
+        ora_xof_finalize(&st);
+        ora_xof_squeeze(&st, ctilde, 32);
+        ora_challenge(mode, cp, ctilde);
+        ora_ntt(cp);
+        /* z = y + c*s1 */
+        for (j = 0; j < p.l && !rej; j++) {
+            pointwise(z[j], cp, s1[j]);
+            ora_invntt_tomont(z[j]);
+            for (c = 0; c < N; c++) z[j][c] = reduce32(z[j][c] + y[j][c]);
+            if (chknorm(z[j], p.gamma1 - p.beta)) rej = 1;
+        }
+        if (rej) continue;
+        /* r0 = w0 - c*s2 */
+        for (i = 0; i < p.k && !rej; i++) {
+            pointwise(h[i], cp, s2[i]);
+            ora_invntt_tomont(h[i]);
+            for (c = 0; c < N; c++) w0[i][c] = reduce32(w0[i][c] - h[i][c]);
+            if (chknorm(w0[i], p.gamma2 - p.beta)) rej = 1;
+        }
+        if (rej) continue;
+        /* c*t0 */
+        for (i = 0; i < p.k && !rej; i++) {
+            pointwise(h[i], cp, t0[i]);
+            ora_invntt_tomont(h[i]);
+            for (c = 0; c < N; c++) h[i][c] = reduce32(h[i][c]);
+            if (chknorm(h[i], p.gamma2)) rej = 1;
+        }
+        if (rej) continue;
+        for (i = 0; i < p.k; i++)
+            for (c = 0; c < N; c++) {
+                w0[i][c] += h[i][c];
+                h[i][c] = make_hint(&p, w0[i][c], w1[i][c]);
+                nh += h[i][c];
+            }
+        if (nh > p.omega) continue;
+        /* sig = ctilde || z || h */
+        memcpy(sig, ctilde, 32);
+        for (j = 0; j < p.l; j++) pack_offset(sig + 32 + j * p.polyz_packed, z[j], p.gamma1, z_bits(&p));
+        {
+            uint8_t *hs = sig + 32 + p.l * p.polyz_packed;
+            int kk = 0;
+            memset(hs, 0, (size_t)(p.omega + p.k));
+            for (i = 0; i < p.k; i++) {
+                for (c = 0; c < N; c++)
+                    if (h[i][c]) hs[kk++] = (uint8_t)c;
+                hs[p.omega + i] = (uint8_t)kk;
+            }
+        }
+        if (attempts) *attempts = att;
+        return 0;
+    }
+}
+
+int ora_sign(int mode, uint8_t *sig, const uint8_t *m, size_t mlen, const uint8_t *sk, int *attempts) {
+    return ora_sign_rhoprime(mode, sig, m, mlen, sk, NULL, attempts);
+}
+
+/* ---------------------------------------------------------------- verify */
+
+int ora_verify(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen, const uint8_t *pk) {
+    ora_params p;
+    static __thread int32_t mat[MAXK * MAXL * N];
+    int32_t z[MAXL][N], t1[MAXK][N], w1[MAXK][N], cp[N];
+    uint8_t hint[MAXK][N];
+    uint8_t trm[32], mu[64], w1packed[MAXK * 192], c2[32];
+    const uint8_t *hs;
+    ora_xof st;
+    int i, j, c, kk;
+    if (ora_params_get(mode, &p)) return -1;
+    if (siglen != (size_t)p.sig_bytes) return -1;
+    /* hint decode with the ordering / omega / zero-padding checks (src/verify.cu:51-93) */
+    hs = sig + 32 + p.l * p.polyz_packed;
+    memset(hint, 0, sizeof hint);
+    kk = 0;
+    for (i = 0; i < p.k; i++) {
+        if (hs[p.omega + i] < kk || hs[p.omega + i] > p.omega) return -1;
+        for (j = kk; j < hs[p.omega + i]; j++) {
+            if (j > kk && hs[j] <= hs[j - 1]) return -1;
+            hint[i][hs[j]] = 1;
+        }
+        kk = hs[p.omega + i];
+    }
+    for (j = kk; j < p.omega; j++)
+        if (hs[j]) return -1;
+    for (j = 0; j < p.l; j++) {
+        unpack_offset(z[j], sig + 32 + j * p.polyz_packed, p.gamma1, z_bits(&p));
+        if (chknorm(z[j], p.gamma1 - p.beta)) return -1;
+    }
+    /* mu = SHAKE256(SHAKE256(pk, 32) || m, 64) */
+    ora_shake256(trm, 32, pk, (size_t)p.pk_bytes);
+    ora_xof_init(&st, ORA_SHAKE256_RATE);
+    ora_xof_absorb(&st, trm, 32);
+    ora_xof_absorb(&st, m, mlen);
+    ora_xof_finalize(&st);
+    ora_xof_squeeze(&st, mu, 64);
+    ora_challenge(mode, cp, sig);
+    ora_expand_a(mode, mat, pk);
+    for (j = 0; j < p.l; j++) ora_ntt(z[j]);
+    ora_ntt(cp);
+    for (i = 0; i < p.k; i++) {
+        uint32_t v[N];
+        int32_t tmp[N];
+        unpack_bits(v, pk + 32 + i * 320, N, 10);
+        for (c = 0; c < N; c++) t1[i][c] = (int32_t)(v[c] << D);
+        ora_ntt(t1[i]);
+        memset(w1[i], 0, sizeof w1[i]);
+        for (j = 0; j < p.l; j++) {
+            pointwise(tmp, mat + (size_t)(i * p.l + j) * N, z[j]);
+            for (c = 0; c < N; c++) w1[i][c] += tmp[c];
+        }
+        pointwise(tmp, cp, t1[i]);
+        for (c = 0; c < N; c++) w1[i][c] = reduce32(w1[i][c] - tmp[c]);
+        ora_invntt_tomont(w1[i]);
+        for (c = 0; c < N; c++) w1[i][c] = use_hint(&p, caddq(w1[i][c]), hint[i][c]);
+        pack_w1(&p, w1packed + i * p.polyw1_packed, w1[i]);
+    }
+    ora_xof_init(&st, ORA_SHAKE256_RATE);
+    ora_xof_absorb(&st, mu, 64);
+    ora_xof_absorb(&st, w1packed, (size_t)p.k * p.polyw1_packed);
+    ora_xof_finalize(&st);
+    ora_xof_squeeze(&st, c2, 32);
+    for (i = 0; i < 32; i++)
+        if (c2[i] != sig[i]) return -1;
+    return 0;
+}
+
+/* ---------------------------------------------------------------- batches */
+
+static int resolve_threads(int nthreads) {
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+    return nthreads;
+#else
+    (void)nthreads;
+    return 1;
+#endif
+}
+
+int ora_keypair_seeds_batch(int mode, uint8_t *pk, uint8_t *sk, const uint8_t *seeds, size_t n, int nthreads) {
+    ora_params p;
+    long i;
+    int bad = 0;
+    if (ora_params_get(mode, &p)) return -1;
+    zetas_init();
+    nthreads = resolve_threads(nthreads);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 8) num_threads(nthreads) reduction(| : bad)
+#endif
+    for (i = 0; i < (long)n; i++)
+        bad |= ora_keypair_from_seed(mode, pk + (size_t)i * p.pk_bytes, sk + (size_t)i * p.sk_bytes, seeds + (size_t)i * 32) != 0;
+    return bad ? -1 : 0;
+}
+
+int ora_keypair_batch(int mode, uint8_t *pk, uint8_t *sk, size_t n, uint64_t rand_index, int nthreads) {
+    ora_params p;
+    long i;
+    int bad = 0;
+    if (ora_params_get(mode, &p)) return -1;
+    zetas_init();
+    nthreads = resolve_threads(nthreads);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 8) num_threads(nthreads) reduction(| : bad)
+#endif
+    for (i = 0; i < (long)n; i++) {
+        uint8_t seed[32];
+        ora_seed_from_ctr(seed, rand_index + 2 * (uint64_t)i + 1); /* src/keypair.cu:53-59 */
+        bad |= ora_keypair_from_seed(mode, pk + (size_t)i * p.pk_bytes, sk + (size_t)i * p.sk_bytes, seed) != 0;
+    }
+    return bad ? -1 : 0;
+}
+
+int ora_sign_batch(int mode, uint8_t *sig, size_t sig_pitch, const uint8_t *m, size_t m_pitch,
+                   const uint64_t *mlens, const uint8_t *sk, size_t sk_pitch, size_t n, int nthreads,
+                   int32_t *attempts) {
+    ora_params p;
+    long i;
+    int bad = 0;
+    if (ora_params_get(mode, &p)) return -1;
+    zetas_init();
+    nthreads = resolve_threads(nthreads);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads) reduction(| : bad)
+#endif
+    for (i = 0; i < (long)n; i++) {
+        int att = 0;
+        bad |= ora_sign(mode, sig + (size_t)i * sig_pitch, m + (size_t)i * m_pitch, (size_t)mlens[i],
+                        sk + (size_t)i * sk_pitch, &att) != 0;
+        if (attempts) attempts[i] = att;
+    }
+    return bad ? -1 : 0;
+}
+
+int ora_verify_batch(int mode, int32_t *ret, const uint8_t *sig, size_t sig_pitch, size_t siglen,
+                     const uint8_t *m, size_t m_pitch, const uint64_t *mlens, const uint8_t *pk, size_t pk_pitch,
+                     size_t n, int nthreads) {
+    ora_params p;
+    long i;
+    if (ora_params_get(mode, &p)) return -1;
+    zetas_init();
+    nthreads = resolve_threads(nthreads);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 8) num_threads(nthreads)
+#endif
+    for (i = 0; i < (long)n; i++)
+        ret[i] = ora_verify(mode, sig + (size_t)i * sig_pitch, siglen, m + (size_t)i * m_pitch, (size_t)mlens[i],
+                            pk + (size_t)i * pk_pitch);
+    return 0;
+}
+
+/* ---------------------------------------------------------------- test vectors */
+
+static size_t put_hex(char *o, const uint8_t *b, size_t n) {
+    static const char hx[] = "0123456789abcdef";
+    size_t i;
+    for (i = 0; i < n; i++) {
+        o[2 * i] = hx[b[i] >> 4];
+        o[2 * i + 1] = hx[b[i] & 15];
+    }
+    return 2 * n;
+}
+
+/* Writes the reference's tvecs<mode> file (tests/test_vectors.cu:40-217) into buf and
+ * returns its length; with buf == NULL (or too small) returns the negated length needed. */
+long ora_tvecs(int mode, size_t nvec, char *buf, size_t buflen, int nthreads) {
+    ora_params p;
+    uint8_t *pk, *sk, *m, *sig;
+    uint64_t *mlens;
+    int32_t *ret;
+    size_t i, need = 0, off = 0;
+    char *out;
+    if (ora_params_get(mode, &p)) return 0;
+    pk = malloc(nvec * p.pk_bytes);
+    sk = malloc(nvec * p.sk_bytes);
+    m = malloc(nvec * 32);
+    sig = malloc(nvec * p.sig_bytes);
+    mlens = malloc(nvec * sizeof *mlens);
+    ret = malloc(nvec * sizeof *ret);
+    for (i = 0; i < nvec; i++) {
+        uint8_t b[8];
+        int j;
+        for (j = 0; j < 8; j++) b[j] = (uint8_t)((uint64_t)(2 * i) >> (8 * j));
+        ora_shake128(m + 32 * i, 32, b, 8); /* tests/test_vectors.cu:58-60 */
+        mlens[i] = 32;
+    }
+    ora_keypair_batch(mode, pk, sk, nvec, 0, nthreads);
+    ora_sign_batch(mode, sig, p.sig_bytes, m, 32, mlens, sk, p.sk_bytes, nvec, nthreads, NULL);
+    ora_verify_batch(mode, ret, sig, p.sig_bytes, p.sig_bytes, m, 32, mlens, pk, p.pk_bytes, nvec, nthreads);
+    out = malloc(nvec * 400 + 64);
+    for (i = 0; i < nvec; i++)
+        if (ret[i]) off += (size_t)sprintf(out + off, "Signature verification failed! %u\n", (unsigned)i);
+    for (i = 0; i < nvec; i++) {
+        uint8_t d[32];
+        off += (size_t)sprintf(out + off, "count = %u\nm = ", (unsigned)i);
+        off += put_hex(out + off, m + 32 * i, 32);
+        off += (size_t)sprintf(out + off, "\npk = ");
+        ora_shake256(d, 32, pk + i * p.pk_bytes, (size_t)p.pk_bytes);
+        off += put_hex(out + off, d, 32);
+        off += (size_t)sprintf(out + off, "\nsk = ");
+        ora_shake256(d, 32, sk + i * p.sk_bytes, (size_t)p.sk_bytes);
+        off += put_hex(out + off, d, 32);
+        off += (size_t)sprintf(out + off, "\nsig = ");
+        ora_shake256(d, 32, sig + i * p.sig_bytes, (size_t)p.sig_bytes);
+        off += put_hex(out + off, d, 32);
+        out[off++] = '\n';
+    }
+    need = off;
+    if (buf && buflen >= need) memcpy(buf, out, need);
+    free(out);
+    free(pk);
+    free(sk);
+    free(m);
+    free(sig);
+    free(mlens);
+    free(ret);
+    if (!buf || buflen < need) return -(long)need;
+    return (long)need;
+}
