@@ -1,0 +1,109 @@
+"""ctypes binding of the in-tree CUDA library (C ABI of ``include/cudilithium.h``).
+
+There is no fallback: if ``libcudilithium_b200.so`` is missing or fails to load, importing this
+module raises, so nothing can silently run on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_int, c_int32, c_size_t, c_uint8, c_uint16, c_uint32, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libcudilithium_b200.so"
+
+CUDIL_OK = 0
+CUDIL_ERR_INVALID = -1
+CUDIL_ERR_CUDA = -2
+CUDIL_ERR_TIMEOUT = -3
+CUDIL_ERR_BUDGET = -4
+
+_ERRORS = {
+    CUDIL_ERR_INVALID: "invalid argument",
+    CUDIL_ERR_CUDA: "CUDA error",
+    CUDIL_ERR_TIMEOUT: "device wait timed out",
+    CUDIL_ERR_BUDGET: "device-memory budget exceeded",
+}
+
+
+class CudilError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what}: {_ERRORS.get(code, 'error')} ({code})")
+        self.code = code
+
+
+class cudil_params(ctypes.Structure):
+    _fields_ = [(n, c_int) for n in (
+        "mode", "k", "l", "eta", "tau", "beta", "gamma1", "gamma2", "omega",
+        "pk_bytes", "sk_bytes", "sig_bytes", "polyz_packed", "polyw1_packed", "polyeta_packed")]
+
+
+class cudil_sign_lut_element(ctypes.Structure):
+    _fields_ = [("done_flag", c_int32), ("nonce", c_uint16)]
+
+
+class cudil_copy_lut_element(ctypes.Structure):
+    _fields_ = [("exec_idx", c_size_t), ("sign_idx", c_size_t)]
+
+
+class cudil_task_lut(ctypes.Structure):
+    _fields_ = [
+        ("sign_lut", POINTER(cudil_sign_lut_element)),
+        ("sign_lut_len", c_size_t),
+        ("h_exec_lut", c_void_p),
+        ("h_done_lut", c_void_p),
+        ("h_copy_lut", c_void_p),
+        ("d_exec_lut", c_void_p),
+        ("d_done_lut", c_void_p),
+        ("d_copy_lut", c_void_p),
+    ]
+
+
+# Every symbol the public header declares, with its ctypes signature.
+SIGNATURES = {
+    "cudil_version": (c_char_p, []),
+    "cudil_get_params": (c_int, [c_int, POINTER(cudil_params)]),
+    "cudil_keypair_row_bytes": (c_size_t, [c_int]),
+    "cudil_sign_row_bytes": (c_size_t, [c_int, c_size_t]),
+    "cudil_sign_temp_row_bytes": (c_size_t, [c_int]),
+    "cudil_verify_row_bytes": (c_size_t, [c_int, c_size_t]),
+    "cudil_keypair": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t]),
+    "cudil_keypair_from_seed": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
+    "cudil_keypair_dev": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t]),
+    "cudil_sign": (c_int, [c_int, c_void_p, c_size_t, POINTER(c_size_t), c_void_p, c_size_t, c_size_t, c_void_p,
+                           c_void_p, c_size_t, c_void_p, c_size_t, POINTER(cudil_task_lut), c_size_t, c_size_t,
+                           c_void_p]),
+    "cudil_sign_dev": (c_int, [c_int, c_void_p, c_size_t, c_void_p, c_size_t, c_size_t, c_void_p, c_void_p, c_size_t,
+                               c_void_p, c_size_t, POINTER(cudil_task_lut), c_size_t, c_size_t, c_void_p]),
+    "cudil_verify": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t, c_void_p,
+                             c_void_p, c_size_t, c_size_t, c_void_p]),
+    "cudil_verify_dev": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
+                                 c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
+    "cudil_ntt_mul": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+}
+
+
+def _load() -> ctypes.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m cudilithium_b200.build` "
+            "(the CUDA path has no CPU fallback)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(code: int, what: str) -> None:
+    if code != CUDIL_OK:
+        raise CudilError(code, what)
+
+
+def params(mode: int) -> cudil_params:
+    p = cudil_params()
+    check(lib.cudil_get_params(mode, ctypes.byref(p)), f"cudil_get_params({mode})")
+    return p

@@ -1,0 +1,165 @@
+// extern "C" boundary: run-time parameter-set dispatch onto the per-mode instantiations, pool row
+// size queries, and the NTT microbenchmark kernel.
+#include <cuda_runtime.h>
+
+#include "../../include/cudilithium.h"
+#include "host_impl.cuh"
+
+namespace cudil {
+extern template struct Impl<2>;
+extern template struct Impl<3>;
+extern template struct Impl<5>;
+
+// One 16-thread group per polynomial: out = invNTT(NTT(a) o b).
+__global__ void __launch_bounds__(kBlock) k_ntt_mul(const int32_t *a, const int32_t *b, int32_t *out, long long npolys) {
+    __shared__ int32_t sm[kGroupsPerBlock * NTT_SMEM_WORDS];
+    const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    if (p >= npolys) return;
+    Group g = make_group(sm, threadIdx.x >> 4);
+    int32_t x[16], y[16];
+    load16_strided(x, a + p * N, g.t);
+    ntt16(x, g.sm, g.gmask, g.t);
+    load16_contig(y, b + p * N + 16 * g.t);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) x[m] = montmul(x[m], y[m]);
+    intt16(x, g.sm, g.gmask, g.t);
+    store16_strided(out + p * N, x, g.t);
+}
+}  // namespace cudil
+
+using namespace cudil;
+
+#define CUDIL_DISPATCH(mode, call)          \
+    switch (mode) {                         \
+        case 2: {                           \
+            using I = Impl<2>;              \
+            return call;                    \
+        }                                   \
+        case 3: {                           \
+            using I = Impl<3>;              \
+            return call;                    \
+        }                                   \
+        case 5: {                           \
+            using I = Impl<5>;              \
+            return call;                    \
+        }                                   \
+        default:                            \
+            return CUDIL_ERR_INVALID;       \
+    }
+
+#define CUDIL_SIZE_DISPATCH(mode, expr)     \
+    switch (mode) {                         \
+        case 2: {                           \
+            using LY = Layout<2>;           \
+            return expr;                    \
+        }                                   \
+        case 3: {                           \
+            using LY = Layout<3>;           \
+            return expr;                    \
+        }                                   \
+        case 5: {                           \
+            using LY = Layout<5>;           \
+            return expr;                    \
+        }                                   \
+        default:                            \
+            return 0;                       \
+    }
+
+template <int MODE>
+static void fill_params(cudil_params *o) {
+    using PM = P<MODE>;
+    o->mode = MODE;
+    o->k = PM::K;
+    o->l = PM::L;
+    o->eta = PM::ETA;
+    o->tau = PM::TAU;
+    o->beta = PM::BETA;
+    o->gamma1 = PM::GAMMA1;
+    o->gamma2 = PM::GAMMA2;
+    o->omega = PM::OMEGA;
+    o->pk_bytes = PM::PK_BYTES;
+    o->sk_bytes = PM::SK_BYTES;
+    o->sig_bytes = PM::SIG_BYTES;
+    o->polyz_packed = PM::POLYZ_PACKED;
+    o->polyw1_packed = PM::POLYW1_PACKED;
+    o->polyeta_packed = PM::POLYETA_PACKED;
+}
+
+extern "C" {
+
+const char *cudil_version(void) { return "cudilithium_b200 0.1 (Dilithium round 3 v3.1, sm_100a)"; }
+
+int cudil_get_params(int mode, cudil_params *out) {
+    if (!out) return CUDIL_ERR_INVALID;
+    switch (mode) {
+        case 2: fill_params<2>(out); return CUDIL_OK;
+        case 3: fill_params<3>(out); return CUDIL_OK;
+        case 5: fill_params<5>(out); return CUDIL_OK;
+        default: return CUDIL_ERR_INVALID;
+    }
+}
+
+size_t cudil_keypair_row_bytes(int mode) { CUDIL_SIZE_DISPATCH(mode, LY::ref_keypair_row()) }
+size_t cudil_sign_row_bytes(int mode, size_t mlen) { CUDIL_SIZE_DISPATCH(mode, LY::ref_sign_row(mlen)) }
+size_t cudil_sign_temp_row_bytes(int mode) { CUDIL_SIZE_DISPATCH(mode, LY::ref_sign_temp_row()) }
+size_t cudil_verify_row_bytes(int mode, size_t mlen) { CUDIL_SIZE_DISPATCH(mode, LY::ref_verify_row(mlen)) }
+
+int cudil_keypair(int mode, uint8_t *pk, uint8_t *sk, uint8_t *d_pool, size_t pitch, size_t batch, void *stream,
+                  size_t rand_index) {
+    CUDIL_DISPATCH(mode, I::keypair(pk, sk, nullptr, d_pool, pitch, batch, (cudaStream_t)stream, rand_index,
+                                    cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost))
+}
+
+int cudil_keypair_from_seed(int mode, uint8_t *pk, uint8_t *sk, const uint8_t *seeds, uint8_t *d_pool, size_t pitch,
+                            size_t batch, void *stream) {
+    if (!seeds) return CUDIL_ERR_INVALID;
+    CUDIL_DISPATCH(mode, I::keypair(pk, sk, seeds, d_pool, pitch, batch, (cudaStream_t)stream, 0, cudaMemcpyHostToDevice,
+                                    cudaMemcpyDeviceToHost))
+}
+
+int cudil_keypair_dev(int mode, uint8_t *d_pk, uint8_t *d_sk, const uint8_t *d_seeds, uint8_t *d_pool, size_t pitch,
+                      size_t batch, void *stream, size_t rand_index) {
+    CUDIL_DISPATCH(mode, I::keypair(d_pk, d_sk, d_seeds, d_pool, pitch, batch, (cudaStream_t)stream, rand_index,
+                                    cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice))
+}
+
+int cudil_sign(int mode, uint8_t *sig, size_t sig_pitch, size_t *siglen, const uint8_t *m, size_t m_pitch, size_t mlen,
+               const uint8_t *sk, uint8_t *d_sign_pool, size_t sign_pitch, uint8_t *d_temp_pool, size_t temp_pitch,
+               cudil_task_lut *lut, size_t exec_threshold, size_t batch, void *stream) {
+    CUDIL_DISPATCH(mode, I::sign(sig, sig_pitch, siglen, m, m_pitch, mlen, sk, I::PM::SK_BYTES, d_sign_pool, sign_pitch,
+                                 d_temp_pool, temp_pitch, lut, exec_threshold, batch, (cudaStream_t)stream,
+                                 cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost))
+}
+
+int cudil_sign_dev(int mode, uint8_t *d_sig, size_t sig_pitch, const uint8_t *d_m, size_t m_pitch, size_t mlen,
+                   const uint8_t *d_sk, uint8_t *d_sign_pool, size_t sign_pitch, uint8_t *d_temp_pool, size_t temp_pitch,
+                   cudil_task_lut *lut, size_t exec_threshold, size_t batch, void *stream) {
+    CUDIL_DISPATCH(mode, I::sign(d_sig, sig_pitch, nullptr, d_m, m_pitch, mlen, d_sk, I::PM::SK_BYTES, d_sign_pool,
+                                 sign_pitch, d_temp_pool, temp_pitch, lut, exec_threshold, batch, (cudaStream_t)stream,
+                                 cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice))
+}
+
+int cudil_verify(int mode, int *ret, const uint8_t *sig, size_t sig_pitch, size_t siglen, const uint8_t *m,
+                 size_t m_pitch, size_t mlen, const uint8_t *pk, uint8_t *d_pool, size_t pitch, size_t batch,
+                 void *stream) {
+    CUDIL_DISPATCH(mode, I::verify(ret, sig, sig_pitch, siglen, m, m_pitch, mlen, pk, I::PM::PK_BYTES, d_pool, pitch,
+                                   batch, (cudaStream_t)stream, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost))
+}
+
+int cudil_verify_dev(int mode, int *d_ret, const uint8_t *d_sig, size_t sig_pitch, size_t siglen, const uint8_t *d_m,
+                     size_t m_pitch, size_t mlen, const uint8_t *d_pk, uint8_t *d_pool, size_t pitch, size_t batch,
+                     void *stream) {
+    CUDIL_DISPATCH(mode, I::verify(d_ret, d_sig, sig_pitch, siglen, d_m, m_pitch, mlen, d_pk, I::PM::PK_BYTES, d_pool,
+                                   pitch, batch, (cudaStream_t)stream, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice))
+}
+
+int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t npolys, void *stream) {
+    if (npolys == 0) return CUDIL_OK;
+    if (!d_a || !d_b || !d_out) return CUDIL_ERR_INVALID;
+    const size_t threads = npolys * 16;
+    k_ntt_mul<<<(unsigned)((threads + kBlock - 1) / kBlock), kBlock, 0, (cudaStream_t)stream>>>(d_a, d_b, d_out,
+                                                                                              (long long)npolys);
+    return cudaGetLastError() == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,7 @@
+// Explicit instantiation of the plain batched path for Dilithium3 (one translation unit per
+// parameter set so the three sets compile in parallel).
+#include "host_impl.cuh"
+
+namespace cudil {
+template struct Impl<3>;
+}  // namespace cudil

@@ -1,0 +1,201 @@
+// Forward / inverse NTT over Z_q for one 256-coefficient polynomial held by a group of 16
+// threads (16 coefficients each, two groups per warp).
+//
+// Arithmetic: the same Cooley-Tukey (forward) and Gentleman-Sande (inverse) butterfly network
+// as the reference (src/ntt.cu:58-207, include/ntt.cuh:74-306): every butterfly is
+// a +/- montmul(zeta, b) with the same zeta, and the inverse ends with a multiplication of
+// every coefficient by f = 41978 (src/ntt.cu:201-205), so outputs are bit-identical to the
+// reference's radix-8 kernels and to the CPU oracle.
+//
+// Layout (radix-16, one shared-memory transpose per transform instead of two):
+//   forward: in  x[i] = a[t + 16 i]  -> levels len 128..16 in registers
+//            transpose through shared memory (17-word padded rows, conflict-free)
+//            levels len 8..1 in registers -> out x[i] = a_hat[16 t + i]
+//   inverse: in  x[i] = a_hat[16 t + i] -> levels len 1..8, transpose, len 16..128, * f
+//            -> out x[i] = a[t + 16 i]
+// so NTT -> pointwise -> invNTT needs no extra exchange, NTT-domain data is stored in natural
+// order with 64 contiguous bytes per thread (128-bit accesses) and time-domain data with 16
+// consecutive words per i across the group (coalesced).
+#pragma once
+
+#include <cstdint>
+
+#include "arith.cuh"
+
+namespace cudil {
+
+// Per-thread twiddles of the register-local half: 15 (zeta, zeta*qinv) pairs for each group
+// position t, padded to 16 pairs (128 bytes) so a thread reads them with 8 x 128-bit loads.
+struct GroupTwiddles {
+    int2 fwd[16][16];  // levels len 8,4,2,1 of the forward transform
+    int2 inv[16][16];  // levels len 1,2,4,8 of the inverse transform (negated zetas)
+};
+
+__host__ __device__ constexpr GroupTwiddles make_group_twiddles() {
+    GroupTwiddles g{};
+    for (int t = 0; t < 16; ++t) {
+        int n = 0;
+        // forward: len 8: zeta[16+t]; len 4: zeta[32+2t+m]; len 2: zeta[64+4t+m]; len 1: zeta[128+8t+m]
+        g.fwd[t][n++] = int2{kTwiddles.zeta[16 + t], kTwiddles.zeta_q[16 + t]};
+        for (int m = 0; m < 2; ++m) g.fwd[t][n++] = int2{kTwiddles.zeta[32 + 2 * t + m], kTwiddles.zeta_q[32 + 2 * t + m]};
+        for (int m = 0; m < 4; ++m) g.fwd[t][n++] = int2{kTwiddles.zeta[64 + 4 * t + m], kTwiddles.zeta_q[64 + 4 * t + m]};
+        for (int m = 0; m < 8; ++m) g.fwd[t][n++] = int2{kTwiddles.zeta[128 + 8 * t + m], kTwiddles.zeta_q[128 + 8 * t + m]};
+        g.fwd[t][15] = int2{0, 0};
+        n = 0;
+        // inverse: len 1: -zeta[255-8t-m]; len 2: -zeta[127-4t-m]; len 4: -zeta[63-2t-m]; len 8: -zeta[31-t]
+        for (int m = 0; m < 8; ++m) g.inv[t][n++] = int2{kTwiddles.izeta[255 - 8 * t - m], kTwiddles.izeta_q[255 - 8 * t - m]};
+        for (int m = 0; m < 4; ++m) g.inv[t][n++] = int2{kTwiddles.izeta[127 - 4 * t - m], kTwiddles.izeta_q[127 - 4 * t - m]};
+        for (int m = 0; m < 2; ++m) g.inv[t][n++] = int2{kTwiddles.izeta[63 - 2 * t - m], kTwiddles.izeta_q[63 - 2 * t - m]};
+        g.inv[t][n++] = int2{kTwiddles.izeta[31 - t], kTwiddles.izeta_q[31 - t]};
+        g.inv[t][15] = int2{0, 0};
+    }
+    return g;
+}
+
+static __device__ const GroupTwiddles g_group_tw = make_group_twiddles();
+// Uniform twiddles (same for all threads of a group): zeta[1..15] and -zeta[1..15].
+static __constant__ TwiddleTables c_tw = make_twiddles();
+
+// Shared-memory words per group for the transpose (16 rows of 17).
+constexpr int NTT_SMEM_WORDS = 16 * 17;
+
+__device__ __forceinline__ void ct_bfly(int32_t &a, int32_t &b, int32_t z, int32_t zq) {
+    int32_t t = montmul_pre(b, z, zq);
+    b = a - t;
+    a = a + t;
+}
+
+__device__ __forceinline__ void gs_bfly(int32_t &a, int32_t &b, int32_t z, int32_t zq) {
+    int32_t t = a;
+    a = t + b;
+    b = montmul_pre(t - b, z, zq);
+}
+
+__device__ __forceinline__ void load_tw16(int2 (&tw)[16], const int2 *src) {
+    const int4 *p = reinterpret_cast<const int4 *>(src);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        int4 v = __ldg(p + i);
+        tw[2 * i] = make_int2(v.x, v.y);
+        tw[2 * i + 1] = make_int2(v.z, v.w);
+    }
+}
+
+// Forward NTT; sm = this group's NTT_SMEM_WORDS-word region, gmask = this group's lanes.
+__device__ __forceinline__ void ntt16(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
+    // len 128: (i, i+8), zeta[1]
+#pragma unroll
+    for (int i = 0; i < 8; ++i) ct_bfly(x[i], x[i + 8], c_tw.zeta[1], c_tw.zeta_q[1]);
+    // len 64: (i, i+4), zeta[2 + (i>>3)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        if (!(i & 4)) ct_bfly(x[i], x[i + 4], c_tw.zeta[2 + (i >> 3)], c_tw.zeta_q[2 + (i >> 3)]);
+    // len 32: (i, i+2), zeta[4 + (i>>2)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        if (!(i & 2)) ct_bfly(x[i], x[i + 2], c_tw.zeta[4 + (i >> 2)], c_tw.zeta_q[4 + (i >> 2)]);
+    // len 16: (i, i+1), zeta[8 + (i>>1)]
+#pragma unroll
+    for (int i = 0; i < 16; i += 2) ct_bfly(x[i], x[i + 1], c_tw.zeta[8 + (i >> 1)], c_tw.zeta_q[8 + (i >> 1)]);
+
+    // transpose: a[j] lives at sm[j + (j >> 4)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i) sm[t + 17 * i] = x[i];
+    __syncwarp(gmask);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = sm[17 * t + i];
+    __syncwarp(gmask);
+
+    int2 tw[16];
+    load_tw16(tw, g_group_tw.fwd[t]);
+    // len 8: (i, i+8), zeta[16+t]
+#pragma unroll
+    for (int i = 0; i < 8; ++i) ct_bfly(x[i], x[i + 8], tw[0].x, tw[0].y);
+    // len 4: zeta[32 + 2t + (i>>3)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        if (!(i & 4)) ct_bfly(x[i], x[i + 4], tw[1 + (i >> 3)].x, tw[1 + (i >> 3)].y);
+    // len 2: zeta[64 + 4t + (i>>2)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        if (!(i & 2)) ct_bfly(x[i], x[i + 2], tw[3 + (i >> 2)].x, tw[3 + (i >> 2)].y);
+    // len 1: zeta[128 + 8t + (i>>1)]
+#pragma unroll
+    for (int i = 0; i < 16; i += 2) ct_bfly(x[i], x[i + 1], tw[7 + (i >> 1)].x, tw[7 + (i >> 1)].y);
+}
+
+// Inverse NTT including the final multiplication by f (invntt_tomont).
+__device__ __forceinline__ void intt16(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
+    int2 tw[16];
+    load_tw16(tw, g_group_tw.inv[t]);
+    // len 1: block 8t + (i>>1): -zeta[255 - 8t - (i>>1)]
+#pragma unroll
+    for (int i = 0; i < 16; i += 2) gs_bfly(x[i], x[i + 1], tw[i >> 1].x, tw[i >> 1].y);
+    // len 2: -zeta[127 - 4t - (i>>2)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        if (!(i & 2)) gs_bfly(x[i], x[i + 2], tw[8 + (i >> 2)].x, tw[8 + (i >> 2)].y);
+    // len 4: -zeta[63 - 2t - (i>>3)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        if (!(i & 4)) gs_bfly(x[i], x[i + 4], tw[12 + (i >> 3)].x, tw[12 + (i >> 3)].y);
+    // len 8: -zeta[31 - t]
+#pragma unroll
+    for (int i = 0; i < 8; ++i) gs_bfly(x[i], x[i + 8], tw[14].x, tw[14].y);
+
+#pragma unroll
+    for (int i = 0; i < 16; ++i) sm[17 * t + i] = x[i];
+    __syncwarp(gmask);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = sm[t + 17 * i];
+    __syncwarp(gmask);
+
+    // len 16: (i, i+1): -zeta[15 - (i>>1)]
+#pragma unroll
+    for (int i = 0; i < 16; i += 2) gs_bfly(x[i], x[i + 1], c_tw.izeta[15 - (i >> 1)], c_tw.izeta_q[15 - (i >> 1)]);
+    // len 32: -zeta[7 - (i>>2)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        if (!(i & 2)) gs_bfly(x[i], x[i + 2], c_tw.izeta[7 - (i >> 2)], c_tw.izeta_q[7 - (i >> 2)]);
+    // len 64: -zeta[3 - (i>>3)]
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+        if (!(i & 4)) gs_bfly(x[i], x[i + 4], c_tw.izeta[3 - (i >> 3)], c_tw.izeta_q[3 - (i >> 3)]);
+    // len 128: -zeta[1]
+#pragma unroll
+    for (int i = 0; i < 8; ++i) gs_bfly(x[i], x[i + 8], c_tw.izeta[1], c_tw.izeta_q[1]);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = montmul_pre(x[i], F_INV, F_INV_Q);
+}
+
+// 64 contiguous bytes (natural-order NTT-domain slice 16t..16t+15) <-> registers.
+__device__ __forceinline__ void load16_contig(int32_t (&x)[16], const int32_t *p) {
+    const int4 *q = reinterpret_cast<const int4 *>(p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        int4 v = q[i];
+        x[4 * i] = v.x;
+        x[4 * i + 1] = v.y;
+        x[4 * i + 2] = v.z;
+        x[4 * i + 3] = v.w;
+    }
+}
+
+__device__ __forceinline__ void store16_contig(int32_t *p, const int32_t (&x)[16]) {
+    int4 *q = reinterpret_cast<int4 *>(p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = make_int4(x[4 * i], x[4 * i + 1], x[4 * i + 2], x[4 * i + 3]);
+}
+
+// Strided slice a[t + 16 i] <-> registers (coalesced across the group).
+__device__ __forceinline__ void load16_strided(int32_t (&x)[16], const int32_t *poly, int t) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = poly[t + 16 * i];
+}
+
+__device__ __forceinline__ void store16_strided(int32_t *poly, const int32_t (&x)[16], int t) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) poly[t + 16 * i] = x[i];
+}
+
+}  // namespace cudil

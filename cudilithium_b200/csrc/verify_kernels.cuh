@@ -1,0 +1,198 @@
+// Batched verification kernels (reference: gpu_verify, src/verify.cu:28-325, one warp per
+// signature).  Split by stage shape:
+//   k_verify_prepare  one thread per signature: hint-encoding checks (src/verify.cu:51-93),
+//                     tr' = H(pk), mu = H(tr'||m), c = SampleInBall(c~)
+//   k_expand_a        one thread per ExpandA entry (shared with signing)
+//   k_verify_w        16-thread groups: z norm check + NTT(z), NTT(c), A z - c t1 2^d, invNTT,
+//                     UseHint, pack w1'
+//   k_verify_final    one thread per signature: c~' = H(mu||w1') and compare
+#pragma once
+
+#include "sign_kernels.cuh"
+
+namespace cudil {
+
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_verify_prepare(uint8_t *pool, size_t pitch, size_t mlen, int n) {
+    using PM = P<MODE>;
+    using LY = Layout<MODE>;
+    constexpr int K = PM::K, OMEGA = PM::OMEGA;
+    __shared__ __align__(8) uint8_t s_blk[kBlock][SHAKE256_RATE];
+    __shared__ uint32_t s_mask[kBlock][16];
+    const int it = blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= n) return;
+    uint8_t *row = pool + (size_t)it * pitch;
+    uint8_t *aux = row + LY::vf_aux(mlen);
+
+    // hint encoding: per-poly counts non-decreasing and <= OMEGA, positions strictly increasing
+    // inside each poly, unused slots zero
+    int status = 0;
+    {
+        const uint8_t *h = row + LY::VF_SIG + PM::SIG_H;
+        int k = 0;
+        for (int i = 0; i < K && !status; ++i) {
+            const int end = h[OMEGA + i];
+            if (end < k || end > OMEGA) {
+                status = 1;
+                break;
+            }
+            for (int j = k + 1; j < end; ++j)
+                if (h[j] <= h[j - 1]) status = 1;
+            k = end;
+        }
+        if (!status)
+            for (int j = k; j < OMEGA; ++j)
+                if (h[j]) status = 1;
+    }
+
+    uint32_t al[25], ah[25];
+    // tr' = SHAKE256(pk, 32) -> row + VF_TRM (m follows it)
+    AlignedBytes pk{row + LY::VF_PK, PM::PK_BYTES};
+    shake_absorb<SHAKE256_RATE>(al, ah, pk, PM::PK_BYTES);
+    keccak_f1600(al, ah);
+    uint2 *trm = reinterpret_cast<uint2 *>(row + LY::VF_TRM);
+#pragma unroll
+    for (int w = 0; w < 4; ++w) trm[w] = make_uint2(al[w], ah[w]);
+    // mu = SHAKE256(tr' || m, 64)
+    AlignedBytes tm{row + LY::VF_TRM, (long long)(SEEDBYTES + mlen)};
+    shake_absorb<SHAKE256_RATE>(al, ah, tm, (long long)(SEEDBYTES + mlen));
+    keccak_f1600(al, ah);
+    uint2 *mu = reinterpret_cast<uint2 *>(row + LY::vf_mu(mlen));
+#pragma unroll
+    for (int w = 0; w < 8; ++w) mu[w] = make_uint2(al[w], ah[w]);
+
+    uint2 ct[4];
+    ld_lanes(ct, row + LY::VF_SIG);
+    uint32_t *mask = s_mask[threadIdx.x];
+    sample_in_ball<PM::TAU>(ct, s_blk[threadIdx.x], mask);
+    uint4 *mo = reinterpret_cast<uint4 *>(aux);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mo[k] = make_uint4(mask[4 * k], mask[4 * k + 1], mask[4 * k + 2], mask[4 * k + 3]);
+    reinterpret_cast<int *>(aux + 64)[0] = status;
+}
+
+// AV signatures per 128-thread block.  Phase 1 units: (sig, j<L) -> z_hat_j, (sig, L) -> c_hat.
+// Phase 2 units: (sig, i<K) -> w1'_i packed.
+template <int MODE, int AV>
+__global__ void __launch_bounds__(kBlock) k_verify_w(uint8_t *pool, size_t pitch, size_t mlen, int n) {
+    using PM = P<MODE>;
+    using LY = Layout<MODE>;
+    constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA;
+    __shared__ __align__(16) int32_t s_hat[AV][L + 1][N];
+    __shared__ uint32_t s_hint[AV][K][8];
+    __shared__ int32_t sm[kGroupsPerBlock * NTT_SMEM_WORDS];
+    const int gi = threadIdx.x >> 4;
+    Group g = make_group(sm, gi);
+    const int i0 = blockIdx.x * AV;
+
+    for (int q = threadIdx.x; q < AV * K * 8; q += blockDim.x) (&s_hint[0][0][0])[q] = 0;
+    __syncthreads();
+    // hint bitmaps (positions are validated by k_verify_prepare; a bad encoding only needs to not
+    // index out of range here, which byte positions < 256 guarantee)
+    for (int q = threadIdx.x; q < AV * K; q += blockDim.x) {
+        const int a = q / K, i = q % K, it = i0 + a;
+        if (it >= n) continue;
+        const uint8_t *h = pool + (size_t)it * pitch + LY::VF_SIG + PM::SIG_H;
+        const int start = (i == 0) ? 0 : h[OMEGA + i - 1];
+        int end = h[OMEGA + i];
+        if (end > OMEGA) end = OMEGA;
+        for (int j = start; j < end; ++j) atomicOr(&s_hint[a][i][h[j] >> 5], 1u << (h[j] & 31));
+    }
+
+    for (int u = gi; u < AV * (L + 1); u += kGroupsPerBlock) {
+        const int a = u / (L + 1), j = u % (L + 1), it = i0 + a;
+        if (it >= n) continue;
+        uint8_t *row = pool + (size_t)it * pitch;
+        int32_t x[16];
+        if (j < L) {
+            unpack_z_strided<MODE>(x, row + LY::VF_SIG + PM::SIG_Z + (size_t)j * PM::POLYZ_PACKED, g.t);
+            bool bad = false;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) bad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
+            if (group_any(g, bad) && g.t == 0) atomicOr(reinterpret_cast<int *>(row + LY::vf_aux(mlen) + 64), 2);
+        } else {
+            uint32_t masks[16];
+            const uint4 *mi = reinterpret_cast<const uint4 *>(row + LY::vf_aux(mlen));
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                uint4 v = mi[k];
+                masks[4 * k] = v.x;
+                masks[4 * k + 1] = v.y;
+                masks[4 * k + 2] = v.z;
+                masks[4 * k + 3] = v.w;
+            }
+            challenge_strided(x, masks, g.t);
+        }
+        ntt16(x, g.sm, g.gmask, g.t);
+        store16_contig(&s_hat[a][j][16 * g.t], x);
+    }
+    __syncthreads();
+
+    for (int u = gi; u < AV * K; u += kGroupsPerBlock) {
+        const int a = u / K, i = u % K, it = i0 + a;
+        if (it >= n) continue;
+        uint8_t *row = pool + (size_t)it * pitch;
+        // t1_i * 2^d, NTT
+        int32_t t1[16];
+        const uint8_t *t1p = row + LY::VF_PK + SEEDBYTES + (size_t)i * POLYT1_PACKED;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) t1[m] = (int32_t)(get_bits(t1p, (g.t + 16 * m) * 10, 10) << D);
+        ntt16(t1, g.sm, g.gmask, g.t);
+        const int32_t *mat = reinterpret_cast<const int32_t *>(row + LY::vf_mat(mlen)) + (size_t)i * L * N;
+        int32_t acc[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) acc[m] = 0;
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            int32_t av[16], zv[16];
+            load16_contig(av, mat + (size_t)j * N + 16 * g.t);
+            load16_contig(zv, &s_hat[a][j][16 * g.t]);
+#pragma unroll
+            for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], zv[m]);
+        }
+        int32_t cv[16];
+        load16_contig(cv, &s_hat[a][L][16 * g.t]);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m] - montmul(cv[m], t1[m]));
+        intt16(acc, g.sm, g.gmask, g.t);
+        int32_t w1[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int c = g.t + 16 * m;
+            const unsigned hb = (s_hint[a][i][c >> 5] >> (c & 31)) & 1u;
+            w1[m] = use_hint<MODE>(caddq(acc[m]), hb);
+        }
+        int32_t w1c[16];
+        strided_to_contig(g, w1, w1c);
+        uint32_t v[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) v[m] = (uint32_t)w1c[m];
+        pack16_words<PM::W1_BITS>(
+            reinterpret_cast<uint32_t *>(row + LY::vf_mu(mlen) + CRHBYTES + (size_t)i * PM::POLYW1_PACKED + g.t * 2 * PM::W1_BITS), v);
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_verify_final(uint8_t *pool, size_t pitch, size_t mlen, int n) {
+    using PM = P<MODE>;
+    using LY = Layout<MODE>;
+    const int it = blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= n) return;
+    uint8_t *row = pool + (size_t)it * pitch;
+    uint8_t *aux = row + LY::vf_aux(mlen);
+    uint32_t al[25], ah[25];
+    AlignedBytes src{row + LY::vf_mu(mlen), CRHBYTES + PM::W1PACKED_BYTES};
+    shake_absorb<SHAKE256_RATE>(al, ah, src, CRHBYTES + PM::W1PACKED_BYTES);
+    keccak_f1600(al, ah);
+    const uint2 *c = reinterpret_cast<const uint2 *>(row + LY::VF_SIG);
+    bool eq = true;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        const uint2 v = c[w];
+        eq &= (v.x == al[w]) && (v.y == ah[w]);
+    }
+    const int status = reinterpret_cast<const int *>(aux + 64)[0];
+    reinterpret_cast<int *>(aux + 68)[0] = (eq && status == 0) ? 0 : -1;
+}
+
+}  // namespace cudil

@@ -1,0 +1,121 @@
+/*
+ * cudilithium_b200 -- C ABI of the B200 batched Dilithium (round 3, v3.1) engine.
+ *
+ * Plain pointers and sizes only.  `stream` is a cudaStream_t passed as void* (NULL = legacy
+ * default stream).  Host buffers should be pinned (cudaMallocHost) for asynchronous copies.
+ * The parameter set is a run-time argument `mode` in {2, 3, 5}.
+ *
+ * Drop-in entry points (same argument meaning, ownership and error behaviour as the reference's
+ * include/api.cuh:27-63, which has one compile-time mode per library):
+ *   cudil_keypair  <-> crypto_sign_keypair    (include/api.cuh:27-29, src/api.cu:26-61)
+ *   cudil_sign     <-> crypto_sign_signature  (include/api.cuh:51-56, src/api.cu:63-452)
+ *   cudil_verify   <-> crypto_sign_verify     (include/api.cuh:58-63, src/api.cu:454-515)
+ * The per-mode C++ signatures of api.cuh are provided by include/api.cuh in this repository,
+ * implemented on top of these functions.
+ */
+#ifndef CUDILITHIUM_B200_H
+#define CUDILITHIUM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CUDIL_OK 0
+#define CUDIL_ERR_INVALID (-1)   /* bad mode, size, pitch or pointer */
+#define CUDIL_ERR_CUDA (-2)      /* a CUDA call or kernel launch failed */
+#define CUDIL_ERR_TIMEOUT (-3)   /* a bounded device wait gave up (fused engine) */
+#define CUDIL_ERR_BUDGET (-4)    /* request exceeds the engine's device-memory budget */
+
+typedef struct {
+    int mode, k, l, eta, tau, beta, gamma1, gamma2, omega;
+    int pk_bytes, sk_bytes, sig_bytes;
+    int polyz_packed, polyw1_packed, polyeta_packed;
+} cudil_params;
+
+/* Layout-compatible with the reference's sign_lut_element / copy_lut_element
+ * (include/api.cuh:31-39). */
+typedef struct {
+    int32_t done_flag;
+    uint16_t nonce;
+} cudil_sign_lut_element;
+
+typedef struct {
+    size_t exec_idx;
+    size_t sign_idx;
+} cudil_copy_lut_element;
+
+/* The reference's task_lut (include/api.cuh:41-49) with the std::vector replaced by
+ * pointer + length.  All arrays are caller-allocated: sign_lut[sign_lut_len] on the host
+ * (sign_lut_len must equal batch_size), h_* pinned host arrays and d_* device arrays of
+ * exec_threshold entries each. */
+typedef struct {
+    cudil_sign_lut_element *sign_lut;
+    size_t sign_lut_len;
+    uint32_t *h_exec_lut;
+    uint8_t *h_done_lut;
+    cudil_copy_lut_element *h_copy_lut;
+    uint32_t *d_exec_lut;
+    uint8_t *d_done_lut;
+    cudil_copy_lut_element *d_copy_lut;
+} cudil_task_lut;
+
+/* Library / parameter queries. */
+const char *cudil_version(void);
+int cudil_get_params(int mode, cudil_params *out);
+
+/* Minimum per-item row sizes of the caller-allocated pitched pools.  They equal the reference's
+ * row formulas (tests/test_vectors.cu:62-166), so pools sized for the reference fit. */
+size_t cudil_keypair_row_bytes(int mode);
+size_t cudil_sign_row_bytes(int mode, size_t mlen);
+size_t cudil_sign_temp_row_bytes(int mode);
+size_t cudil_verify_row_bytes(int mode, size_t mlen);
+
+/* Key generation for batch_size keys; seed of key i = SHAKE128(le64(rand_index + 2i + 1))[0:32]
+ * (src/keypair.cu:53-59).  pk/sk: dense host arrays.  Asynchronous on `stream`; returns after
+ * queueing (results valid after the caller synchronizes), as crypto_sign_keypair. */
+int cudil_keypair(int mode, uint8_t *pk, uint8_t *sk, uint8_t *d_keypair_pool, size_t keypair_pool_pitch,
+                  size_t batch_size, void *stream, size_t rand_index);
+
+/* Key generation from caller-provided 32-byte seeds (seeds: dense host array). */
+int cudil_keypair_from_seed(int mode, uint8_t *pk, uint8_t *sk, const uint8_t *seeds, uint8_t *d_keypair_pool,
+                            size_t keypair_pool_pitch, size_t batch_size, void *stream);
+
+/* Deterministic signing of batch_size messages of mlen bytes; the signature of each item is the
+ * one of the smallest nonce whose attempt is accepted.  Synchronizes `stream` once per rejection
+ * round (as the reference, src/api.cu:307-310); the final signature copy is asynchronous. */
+int cudil_sign(int mode, uint8_t *sig, size_t sig_pitch, size_t *siglen, const uint8_t *m, size_t m_pitch,
+               size_t mlen, const uint8_t *sk, uint8_t *d_sign_pool, size_t sign_pool_pitch, uint8_t *d_temp_pool,
+               size_t temp_pool_pitch, cudil_task_lut *lut, size_t exec_threshold, size_t batch_size, void *stream);
+
+/* ret[i] = 0 if signature i is valid for (m_i, pk_i), else -1.  siglen != sig_bytes sets every
+ * ret[i] = -1 without touching the GPU (src/api.cu:461-464).  Asynchronous on `stream`. */
+int cudil_verify(int mode, int *ret, const uint8_t *sig, size_t sig_pitch, size_t siglen, const uint8_t *m,
+                 size_t m_pitch, size_t mlen, const uint8_t *pk, uint8_t *d_verify_pool, size_t verify_pool_pitch,
+                 size_t batch_size, void *stream);
+
+/* Device-resident variants: every data pointer is device memory (m, sk, pk, sig, seeds, ret),
+ * nothing crosses PCIe except the sign scheduler's per-round flags. */
+int cudil_keypair_dev(int mode, uint8_t *d_pk, uint8_t *d_sk, const uint8_t *d_seeds, uint8_t *d_keypair_pool,
+                      size_t keypair_pool_pitch, size_t batch_size, void *stream, size_t rand_index);
+int cudil_sign_dev(int mode, uint8_t *d_sig, size_t sig_pitch, const uint8_t *d_m, size_t m_pitch, size_t mlen,
+                   const uint8_t *d_sk, uint8_t *d_sign_pool, size_t sign_pool_pitch, uint8_t *d_temp_pool,
+                   size_t temp_pool_pitch, cudil_task_lut *lut, size_t exec_threshold, size_t batch_size,
+                   void *stream);
+int cudil_verify_dev(int mode, int *d_ret, const uint8_t *d_sig, size_t sig_pitch, size_t siglen, const uint8_t *d_m,
+                     size_t m_pitch, size_t mlen, const uint8_t *d_pk, uint8_t *d_verify_pool,
+                     size_t verify_pool_pitch, size_t batch_size, void *stream);
+
+/* NTT microbenchmark (no reference API counterpart; replaces benches/bench_ntt_radix{2,8}.cu):
+ * d_out[p] = invNTT(NTT(d_a[p]) o d_b[p]) for npolys polynomials of 256 int32, Montgomery
+ * pointwise product, bit-exact with the oracle's ntt / poly_pointwise_montgomery /
+ * invntt_tomont.  d_out may alias d_a. */
+int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t npolys, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,88 @@
+"""The CPU oracle against the reference's pinned golden values (no GPU)."""
+import hashlib
+import os
+import random
+
+import numpy as np
+import pytest
+
+MODES = [2, 3, 5]
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_oracle_reproduces_reference_tvecs_digest(oracle, golden_digests, mode):
+    """sha256 of the regenerated tvecs file equals the reference's CTest digest."""
+    data = oracle.tvecs(mode, golden_digests["nvectors"])
+    assert hashlib.sha256(data).hexdigest() == golden_digests["sha256"][str(mode)]
+
+
+def test_keccak_matches_hashlib(oracle):
+    rng = random.Random(7)
+    for n in [0, 1, 7, 33, 135, 136, 137, 167, 168, 169, 271, 272, 1000]:
+        data = bytes(rng.getrandbits(8) for _ in range(n))
+        for outlen in [1, 32, 136, 168, 500]:
+            assert oracle.shake128(data, outlen) == hashlib.shake_128(data).digest(outlen)
+            assert oracle.shake256(data, outlen) == hashlib.shake_256(data).digest(outlen)
+
+
+def test_keccak_matches_reference_fips202(oracle):
+    """Byte-for-byte against the reference's own src/fips202/fips202.c compiled into oracle/_ref."""
+    import ctypes
+    if not oracle.REF_LIB.exists():
+        if oracle.REF_SRC.exists():
+            oracle.build(ref=True)
+        else:
+            pytest.skip("reference fips202.c not available here")
+    ref = ctypes.CDLL(str(oracle.REF_LIB))
+    rng = random.Random(11)
+    for n in [0, 3, 136, 168, 333, 2000]:
+        data = bytes(rng.getrandbits(8) for _ in range(n))
+        for outlen in [32, 64, 840]:
+            a = ctypes.create_string_buffer(outlen)
+            ref.shake128(a, ctypes.c_size_t(outlen), data, ctypes.c_size_t(n))
+            assert oracle.shake128(data, outlen) == a.raw
+            ref.shake256(a, ctypes.c_size_t(outlen), data, ctypes.c_size_t(n))
+            assert oracle.shake256(data, outlen) == a.raw
+
+
+def test_ntt_roundtrip_and_product(oracle):
+    """invNTT(NTT(a) o mont^2-ish) identities: NTT->invNTT multiplies by 2^32 mod q (tomont)."""
+    q = 8380417
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, q, 256, dtype=np.int64).astype(np.int32)
+    r = oracle.invntt_tomont(oracle.ntt(a)).astype(np.int64)
+    mont = (1 << 32) % q
+    assert np.all((r - a.astype(np.int64) * mont) % q == 0)
+    # schoolbook negacyclic product vs NTT product: invNTT(NTT(a) o NTT(b)) = a*b (mod q, x^256+1)
+    b = rng.integers(-4, 5, 256, dtype=np.int64).astype(np.int32)
+    ah, bh = oracle.ntt(a), oracle.ntt(b)
+    prod = oracle.ntt_mul_batch(a[None, :], bh[None, :])[0].astype(np.int64)
+    ref = np.zeros(256, dtype=object)
+    for i in range(256):
+        for j in range(256):
+            k = i + j
+            v = int(a[i]) * int(b[j])
+            if k >= 256:
+                ref[k - 256] -= v
+            else:
+                ref[k] += v
+    ref = np.array([int(x) % q for x in ref], dtype=np.int64)
+    assert np.all((prod - ref) % q == 0)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_oracle_negative_cases(oracle, mode):
+    p = oracle.params(mode)
+    m = oracle.messages_from_ctr(6, 48)
+    pk, sk = oracle.keypair_batch(mode, 6, rand_index=100)
+    sig = oracle.sign_batch(mode, m, sk)
+    assert np.all(oracle.verify_batch(mode, sig, m, pk) == 0)
+    bad = sig.copy()
+    bad[0, 5] ^= 1          # c~
+    bad[1, 100] ^= 0x10     # z
+    bad[2, p.sig_bytes - 1] = 0xFF  # omega count out of range
+    m2 = m.copy()
+    m2[3, 0] ^= 1
+    ret = oracle.verify_batch(mode, bad, m2, pk)
+    assert list(ret[:4]) == [-1, -1, -1, -1]
+    assert np.all(oracle.verify_batch(mode, sig, m, pk, siglen=p.sig_bytes - 1) == -1)
