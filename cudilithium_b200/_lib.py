@@ -79,13 +79,20 @@ SIGNATURES = {
     "cudil_verify_dev": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
                                  c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
     "cudil_ntt_mul": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "cudil_alu_peak": (c_int, [c_void_p, c_int, c_int, c_void_p, POINTER(ctypes.c_double)]),
+    "cudil_launch_count": (ctypes.c_ulonglong, []),
+    "cudil_kernel_timing": (None, [c_int]),
+    "cudil_kernel_count": (c_int, []),
+    "cudil_kernel_name": (c_char_p, [c_int]),
+    "cudil_kernel_stats": (c_int, [c_int, POINTER(ctypes.c_double), POINTER(ctypes.c_ulonglong)]),
+    "cudil_kernel_stats_reset": (None, []),
 }
 
 
 def _load() -> ctypes.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m cudilithium_b200.build` "
+            f"{LIB_PATH} is missing: build it with `python cudilithium_b200/build.py` "
             "(the CUDA path has no CPU fallback)")
     lib = ctypes.CDLL(str(LIB_PATH))
     for name, (res, args) in SIGNATURES.items():
@@ -101,6 +108,17 @@ lib = _load()
 def check(code: int, what: str) -> None:
     if code != CUDIL_OK:
         raise CudilError(code, what)
+
+
+def kernel_stats() -> dict:
+    """{kernel name: (total device ms, launches)} accumulated while cudil_kernel_timing(1) was on."""
+    out = {}
+    for i in range(lib.cudil_kernel_count()):
+        ms, n = ctypes.c_double(0), ctypes.c_ulonglong(0)
+        lib.cudil_kernel_stats(i, ctypes.byref(ms), ctypes.byref(n))
+        if n.value:
+            out[lib.cudil_kernel_name(i).decode()] = (ms.value, n.value)
+    return out
 
 
 def params(mode: int) -> cudil_params:

@@ -2,7 +2,8 @@
 
 Each ``csrc/*.cu`` translation unit (one per Dilithium parameter set plus the C-ABI unit) is
 compiled in parallel with nvcc and linked into one shared library that exports the C ABI
-declared in ``include/cudilithium.h``.  Run ``python -m cudilithium_b200.build``.
+declared in ``include/cudilithium.h``.  Run ``python cudilithium_b200/build.py`` (by path: importing
+the package would load the library being built).
 """
 from __future__ import annotations
 

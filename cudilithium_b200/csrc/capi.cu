@@ -4,11 +4,36 @@
 
 #include "../../include/cudilithium.h"
 #include "host_impl.cuh"
+#include "profiling.cuh"
 
 namespace cudil {
 extern template struct Impl<2>;
 extern template struct Impl<3>;
 extern template struct Impl<5>;
+
+// Peak of the 32-bit logic/shift mix that Keccak-f[1600] issues (3 LOP3 : 1 funnel shift, the
+// ratio of a LOP3/SHF lowering of theta/rho/chi): 8 independent chains per thread.
+__global__ void __launch_bounds__(256) k_alu_peak(uint32_t *out, int iters) {
+    uint32_t a[8];
+    const uint32_t b = threadIdx.x * 0x9E3779B9u + 1u, c = blockIdx.x * 0x7F4A7C15u + 3u;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = threadIdx.x + (uint32_t)k * 0x01234567u;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            uint32_t x = a[k];
+            asm("lop3.b32 %0, %0, %1, %2, 0x96;" : "+r"(x) : "r"(b), "r"(c));
+            asm("lop3.b32 %0, %0, %1, %2, 0xD2;" : "+r"(x) : "r"(c), "r"(b));
+            asm("lop3.b32 %0, %0, %1, %2, 0x78;" : "+r"(x) : "r"(b), "r"(c));
+            asm("shf.l.wrap.b32 %0, %0, %1, 7;" : "+r"(x) : "r"(b));
+            a[k] = x;
+        }
+    }
+    uint32_t r = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r ^= a[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = r;
+}
 
 // One 16-thread group per polynomial: out = invNTT(NTT(a) o b).
 __global__ void __launch_bounds__(kBlock) k_ntt_mul(const int32_t *a, const int32_t *b, int32_t *out, long long npolys) {
@@ -157,9 +182,40 @@ int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t
     if (npolys == 0) return CUDIL_OK;
     if (!d_a || !d_b || !d_out) return CUDIL_ERR_INVALID;
     const size_t threads = npolys * 16;
-    k_ntt_mul<<<(unsigned)((threads + kBlock - 1) / kBlock), kBlock, 0, (cudaStream_t)stream>>>(d_a, d_b, d_out,
-                                                                                              (long long)npolys);
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDIL_LAUNCH(KID_NTT_MUL, st,
+                 k_ntt_mul<<<(unsigned)((threads + kBlock - 1) / kBlock), kBlock, 0, st>>>(d_a, d_b, d_out, (long long)npolys));
     return cudaGetLastError() == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
 }
+
+int cudil_alu_peak(uint32_t *d_out, int blocks, int iters, void *stream, double *ops_per_launch) {
+    if (!d_out || blocks <= 0 || iters <= 0) return CUDIL_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDIL_LAUNCH(KID_ALU_PEAK, st, k_alu_peak<<<blocks, 256, 0, st>>>(d_out, iters));
+    if (ops_per_launch) *ops_per_launch = (double)blocks * 256.0 * iters * 8.0 * 4.0;
+    return cudaGetLastError() == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
+}
+
+unsigned long long cudil_launch_count(void) { return Profiler::get().launches.load(); }
+
+void cudil_kernel_timing(int enable) {
+    Profiler::get().collect();
+    Profiler::get().timing.store(enable ? 1 : 0);
+}
+
+int cudil_kernel_count(void) { return KID_COUNT; }
+
+const char *cudil_kernel_name(int id) { return kernel_name(id); }
+
+int cudil_kernel_stats(int id, double *total_ms, unsigned long long *launches) {
+    if (id < 0 || id >= KID_COUNT) return CUDIL_ERR_INVALID;
+    Profiler &p = Profiler::get();
+    p.collect();
+    if (total_ms) *total_ms = p.total_ms[id];
+    if (launches) *launches = p.count[id];
+    return CUDIL_OK;
+}
+
+void cudil_kernel_stats_reset(void) { Profiler::get().reset(); }
 
 }  // extern "C"

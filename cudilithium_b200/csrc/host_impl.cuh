@@ -7,11 +7,13 @@
 
 #include <climits>
 #include <cstring>
+#include <vector>
 
 #include <cuda_runtime.h>
 
 #include "../../include/cudilithium.h"
 #include "keypair_kernels.cuh"
+#include "profiling.cuh"
 #include "verify_kernels.cuh"
 
 namespace cudil {
@@ -58,13 +60,13 @@ struct Impl {
         const int nn = (int)n;
         CUDIL_CK(cudaMemset2DAsync(pool + LY::KP_TACC, pitch, 0, (size_t)K * LY::POLY, n, st));
         if (seeds) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::KP_SK + PM::SK_TR, pitch, seeds, SEEDBYTES, SEEDBYTES, n, in_kind, st));
-        k_kp_seed<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, nn, (unsigned long long)rand_index, seeds ? 1 : 0);
+        CUDIL_LAUNCH(KID_KP_SEED, st, k_kp_seed<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, nn, (unsigned long long)rand_index, seeds ? 1 : 0));
         CUDIL_CK_LAUNCH();
         const size_t smem = KpSmem<MODE>::bytes(KPI);
         CUDIL_CK(cudaFuncSetAttribute(k_kp_main<MODE, KPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_kp_main<MODE, KPI><<<(unsigned)((n + KPI - 1) / KPI), kBlock, smem, st>>>(pool, pitch, nn);
+        CUDIL_LAUNCH(KID_KP_MAIN, st, k_kp_main<MODE, KPI><<<(unsigned)((n + KPI - 1) / KPI), kBlock, smem, st>>>(pool, pitch, nn));
         CUDIL_CK_LAUNCH();
-        k_kp_tr<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, nn);
+        CUDIL_LAUNCH(KID_KP_TR, st, k_kp_tr<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_CK(cudaMemcpy2DAsync(pk, PM::PK_BYTES, pool + LY::KP_PK, pitch, PM::PK_BYTES, n, out_kind, st));
         CUDIL_CK(cudaMemcpy2DAsync(sk, PM::SK_BYTES, pool + LY::KP_SK, pitch, PM::SK_BYTES, n, out_kind, st));
@@ -77,11 +79,11 @@ struct Impl {
         const int nn = (int)n;
         if (mlen) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::SG_MSG, sp, m, m_pitch, mlen, n, in_kind, st));
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::SG_SK, sp, sk, sk_pitch, PM::SK_BYTES, n, in_kind, st));
-        k_sign_prehash<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, sp, mlen, nn);
+        CUDIL_LAUNCH(KID_SIGN_PREHASH, st, k_sign_prehash<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, sp, mlen, nn));
         CUDIL_CK_LAUNCH();
-        k_expand_a<MODE><<<blocks_for(n * K * L), kBlock, 0, st>>>(pool, sp, LY::SG_SK + PM::SK_RHO, LY::sg_mat(mlen), nn);
+        CUDIL_LAUNCH(KID_EXPAND_A, st, k_expand_a<MODE><<<blocks_for(n * K * L), kBlock, 0, st>>>(pool, sp, LY::SG_SK + PM::SK_RHO, LY::sg_mat(mlen), nn));
         CUDIL_CK_LAUNCH();
-        k_sign_unpack_ntt<MODE><<<blocks_for(n * (L + 2 * K) * 16), kBlock, 0, st>>>(pool, sp, mlen, nn);
+        CUDIL_LAUNCH(KID_SIGN_UNPACK_NTT, st, k_sign_unpack_ntt<MODE><<<blocks_for(n * (L + 2 * K) * 16), kBlock, 0, st>>>(pool, sp, mlen, nn));
         CUDIL_CK_LAUNCH();
         return CUDIL_OK;
     }
@@ -89,13 +91,13 @@ struct Impl {
     // One rejection round over nexec exec slots (exec LUT already on the device).
     static int sign_round(uint8_t *pool, size_t sp, size_t mlen, uint8_t *tpool, size_t tp, const uint32_t *d_exec,
                           uint8_t *d_done, int nexec, cudaStream_t st) {
-        k_sign_expand_mask<MODE><<<blocks_for((size_t)nexec * L), kBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec);
+        CUDIL_LAUNCH(KID_SIGN_EXPAND_MASK, st, k_sign_expand_mask<MODE><<<blocks_for((size_t)nexec * L), kBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec));
         CUDIL_CK_LAUNCH();
-        k_sign_compute_w<MODE, AW><<<(unsigned)((nexec + AW - 1) / AW), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, nexec);
+        CUDIL_LAUNCH(KID_SIGN_COMPUTE_W, st, k_sign_compute_w<MODE, AW><<<(unsigned)((nexec + AW - 1) / AW), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, nexec));
         CUDIL_CK_LAUNCH();
-        k_sign_challenge<MODE><<<blocks_for((size_t)nexec), kBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec);
+        CUDIL_LAUNCH(KID_SIGN_CHALLENGE, st, k_sign_challenge<MODE><<<blocks_for((size_t)nexec), kBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec));
         CUDIL_CK_LAUNCH();
-        k_sign_reject<MODE><<<blocks_for((size_t)nexec * 16), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, d_done, nexec);
+        CUDIL_LAUNCH(KID_SIGN_REJECT, st, k_sign_reject<MODE><<<blocks_for((size_t)nexec * 16), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, d_done, nexec));
         CUDIL_CK_LAUNCH();
         return CUDIL_OK;
     }
@@ -123,14 +125,22 @@ struct Impl {
         }
         size_t remaining = n;
         size_t rounds = 0;
+        std::vector<uint32_t> pending;
+        pending.reserve(n);
         while (remaining) {
             if (++rounds > (size_t)1 << 20) return CUDIL_ERR_TIMEOUT;
-            // fill every exec slot, cycling over pending items with consecutive nonces
-            // (src/api.cu:221-232 and :322-332)
+            // fill every exec slot, cycling over pending items in index order with consecutive
+            // nonces (the exec order of src/api.cu:221-232 and :322-332); the pending list keeps
+            // the fill linear in T when few items remain
+            pending.clear();
+            for (size_t s = 0; s < n; ++s)
+                if (!sl[s].done_flag) pending.push_back((uint32_t)s);
             size_t e = 0;
             while (e < T) {
-                for (size_t s = 0; s < n && e < T; ++s)
-                    if (!sl[s].done_flag) lut->h_exec_lut[e++] = ((uint32_t)s << 16) | (uint32_t)(sl[s].nonce++);
+                for (size_t q = 0; q < pending.size() && e < T; ++q) {
+                    const uint32_t s = pending[q];
+                    lut->h_exec_lut[e++] = (s << 16) | (uint32_t)(sl[s].nonce++);
+                }
             }
             CUDIL_CK(cudaMemcpyAsync(lut->d_exec_lut, lut->h_exec_lut, sizeof(uint32_t) * T, cudaMemcpyHostToDevice, st));
             CUDIL_CK(cudaMemsetAsync(lut->d_done_lut, 0, T, st));
@@ -153,8 +163,8 @@ struct Impl {
             if (cc) {
                 CUDIL_CK(cudaMemcpyAsync(lut->d_copy_lut, lut->h_copy_lut, sizeof(cudil_copy_lut_element) * cc,
                                          cudaMemcpyHostToDevice, st));
-                k_sig_copy<MODE><<<(unsigned)cc, 128, 0, st>>>(pool, sp, tpool, tp,
-                                                               reinterpret_cast<const CopyEntry *>(lut->d_copy_lut));
+                CUDIL_LAUNCH(KID_SIG_COPY, st, k_sig_copy<MODE><<<(unsigned)cc, 128, 0, st>>>(pool, sp, tpool, tp,
+                                                               reinterpret_cast<const CopyEntry *>(lut->d_copy_lut)));
                 CUDIL_CK_LAUNCH();
             }
         }
@@ -183,13 +193,13 @@ struct Impl {
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::VF_SIG, pitch, sig, sig_pitch, PM::SIG_BYTES, n, in_kind, st));
         if (mlen) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::VF_TRM + SEEDBYTES, pitch, m, m_pitch, mlen, n, in_kind, st));
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::VF_PK, pitch, pk, pk_pitch, PM::PK_BYTES, n, in_kind, st));
-        k_verify_prepare<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, mlen, nn);
+        CUDIL_LAUNCH(KID_VERIFY_PREPARE, st, k_verify_prepare<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, mlen, nn));
         CUDIL_CK_LAUNCH();
-        k_expand_a<MODE><<<blocks_for(n * K * L), kBlock, 0, st>>>(pool, pitch, LY::VF_PK, LY::vf_mat(mlen), nn);
+        CUDIL_LAUNCH(KID_EXPAND_A, st, k_expand_a<MODE><<<blocks_for(n * K * L), kBlock, 0, st>>>(pool, pitch, LY::VF_PK, LY::vf_mat(mlen), nn));
         CUDIL_CK_LAUNCH();
-        k_verify_w<MODE, AV><<<(unsigned)((n + AV - 1) / AV), kBlock, 0, st>>>(pool, pitch, mlen, nn);
+        CUDIL_LAUNCH(KID_VERIFY_W, st, k_verify_w<MODE, AV><<<(unsigned)((n + AV - 1) / AV), kBlock, 0, st>>>(pool, pitch, mlen, nn));
         CUDIL_CK_LAUNCH();
-        k_verify_final<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, mlen, nn);
+        CUDIL_LAUNCH(KID_VERIFY_FINAL, st, k_verify_final<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, mlen, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_CK(cudaMemcpy2DAsync(ret, sizeof(int), pool + LY::vf_aux(mlen) + 68, pitch, sizeof(int), n, out_kind, st));
         return CUDIL_OK;

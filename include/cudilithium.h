@@ -115,6 +115,21 @@ int cudil_verify_dev(int mode, int *d_ret, const uint8_t *d_sig, size_t sig_pitc
  * invntt_tomont.  d_out may alias d_a. */
 int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t npolys, void *stream);
 
+/* Peak of the 32-bit LOP3/funnel-shift mix Keccak-f[1600] issues: launches `blocks` x 256 threads
+ * doing `iters` x 32 ALU operations each; *ops_per_launch receives the operation count. */
+int cudil_alu_peak(uint32_t *d_out, int blocks, int iters, void *stream, double *ops_per_launch);
+
+/* Launch accounting.  cudil_launch_count: kernels launched by this library so far (process-wide).
+ * cudil_kernel_timing(1) brackets every later launch with CUDA events on its stream (off by
+ * default); cudil_kernel_stats returns the accumulated device time and launches of kernel id
+ * (0 <= id < cudil_kernel_count(), named by cudil_kernel_name). */
+unsigned long long cudil_launch_count(void);
+void cudil_kernel_timing(int enable);
+int cudil_kernel_count(void);
+const char *cudil_kernel_name(int id);
+int cudil_kernel_stats(int id, double *total_ms, unsigned long long *launches);
+void cudil_kernel_stats_reset(void);
+
 #ifdef __cplusplus
 }
 #endif
