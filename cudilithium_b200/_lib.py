@@ -79,6 +79,9 @@ SIGNATURES = {
     "cudil_verify_dev": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
                                  c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
     "cudil_ntt_mul": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "cudil_verify_noalloc_max_batch": (c_size_t, [c_int, c_size_t]),
+    "cudil_verify_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
+                                     c_void_p, c_size_t, c_void_p]),
     "cudil_alu_peak": (c_int, [c_void_p, c_int, c_int, c_void_p, POINTER(ctypes.c_double)]),
     "cudil_launch_count": (ctypes.c_ulonglong, []),
     "cudil_kernel_timing": (None, [c_int]),

@@ -109,6 +109,20 @@ int cudil_verify_dev(int mode, int *d_ret, const uint8_t *d_sig, size_t sig_pitc
                      size_t m_pitch, size_t mlen, const uint8_t *d_pk, uint8_t *d_verify_pool,
                      size_t verify_pool_pitch, size_t batch_size, void *stream);
 
+/* Verification without any device allocation, for callers that may not allocate device memory
+ * where they verify (budgeted or pre-reserved device memory, latency-critical threads that must
+ * not hit cudaMalloc/cudaFree, hosts that own every allocation).  No counterpart in the
+ * reference (its crypto_sign_verify needs a caller-allocated pool).  Same arguments and results as
+ * cudil_verify minus the pool: the pool is a fixed CUDIL_NOALLOC_SCRATCH_BYTES array inside the
+ * library, reserved on every GPU that loads it.  At most cudil_verify_noalloc_max_batch(mode,
+ * mlen) signatures per call (larger batches: CUDIL_ERR_BUDGET).  All calls share the array, so
+ * calls that overlap on the GPU race and must be serialized by the caller.  The first call on a
+ * device looks up the array's address; make it before any stream capture. */
+#define CUDIL_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+size_t cudil_verify_noalloc_max_batch(int mode, size_t mlen);
+int cudil_verify_noalloc(int mode, int *ret, const uint8_t *sig, size_t sig_pitch, size_t siglen, const uint8_t *m,
+                         size_t m_pitch, size_t mlen, const uint8_t *pk, size_t batch_size, void *stream);
+
 /* NTT microbenchmark (no reference API counterpart; replaces benches/bench_ntt_radix{2,8}.cu):
  * d_out[p] = invNTT(NTT(d_a[p]) o d_b[p]) for npolys polynomials of 256 int32, Montgomery
  * pointwise product, bit-exact with the oracle's ntt / poly_pointwise_montgomery /
