@@ -82,6 +82,17 @@ SIGNATURES = {
     "cudil_verify_noalloc_max_batch": (c_size_t, [c_int, c_size_t]),
     "cudil_verify_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
                                      c_void_p, c_size_t, c_void_p]),
+    "cudil_engine_create": (c_int, [POINTER(c_void_p), c_int, c_size_t, c_size_t, c_int, c_size_t]),
+    "cudil_engine_destroy": (c_int, [c_void_p]),
+    "cudil_engine_device_bytes": (c_size_t, [c_void_p]),
+    "cudil_engine_set_secret_keys": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
+    "cudil_engine_set_public_keys": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
+    "cudil_engine_sign": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_size_t,
+                                  c_void_p]),
+    "cudil_engine_verify": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p,
+                                    c_size_t, c_void_p]),
+    "cudil_engine_last_status": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong), POINTER(c_uint32)]),
+    "cudil_engine_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "cudil_alu_peak": (c_int, [c_void_p, c_int, c_int, c_void_p, POINTER(ctypes.c_double)]),
     "cudil_launch_count": (ctypes.c_ulonglong, []),
     "cudil_kernel_timing": (None, [c_int]),

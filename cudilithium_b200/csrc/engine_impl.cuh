@@ -1,0 +1,283 @@
+// Host side of the fused engine: device buffers sized once at creation, per-key caches, and the
+// graph that runs a whole signing (or verification) batch on the device with one launch:
+//   [k_fused_init] -> [k_fused_prehash] -> [k_fused_sign]       (sign)
+//   [k_fused_init] -> [k_fused_verify]                           (verify)
+// The batch size travels in device memory (FusedQueue::n), so one instantiated graph serves every
+// batch size up to the engine's capacity; only the per-item metadata upload precedes the launch.
+#pragma once
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "fused_kernels.cuh"
+#include "host_impl.cuh"
+#include "profiling.cuh"
+
+namespace cudil {
+
+struct EngineBase {
+    int mode = 0, threads = 0, device = 0, sm_count = 0;
+    size_t max_keys = 0, max_items = 0;
+    size_t n_sk = 0, n_pk = 0;
+    uint8_t *sk_cache = nullptr, *pk_cache = nullptr;
+    size_t sk_pitch = 0, pk_pitch = 0;
+    uint8_t *items = nullptr;       // max_items * 128
+    unsigned *best = nullptr, *locks = nullptr;
+    FusedQueue *q = nullptr;
+    // metadata (device) and its pinned staging
+    unsigned *d_key = nullptr, *d_mlen = nullptr, *d_order = nullptr;
+    unsigned long long *d_off = nullptr;
+    uint8_t *h_stage = nullptr;     // [FusedQueue | key | mlen | order | off]
+    FusedQueue *h_status = nullptr; // D2H copy of the queue after a batch
+    uint8_t *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int sign_grid = 0, verify_grid = 0, prehash_grid = 0;
+    size_t sign_smem = 0, verify_smem = 0;
+    // instantiated graphs, keyed by the output / message buffers they were captured with
+    cudaGraphExec_t g_sign = nullptr, g_verify = nullptr;
+    const void *g_sign_key[2] = {nullptr, nullptr}, *g_verify_key[2] = {nullptr, nullptr};
+    cudaStream_t g_sign_stream = nullptr, g_verify_stream = nullptr;
+    size_t device_bytes = 0;
+    virtual ~EngineBase() = default;
+};
+
+template <int MODE>
+struct EngineImpl : EngineBase {
+    using PM = P<MODE>;
+    using C = Cache<MODE>;
+
+    static size_t stage_bytes(size_t max_items) {
+        return 64 + max_items * (3 * sizeof(unsigned) + sizeof(unsigned long long));
+    }
+
+    template <int T>
+    static int grid_for(const void *fn, size_t smem, int sm_count) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, T, smem) != cudaSuccess || per_sm < 1) return 0;
+        return per_sm * sm_count;
+    }
+
+    // Device bytes the engine needs (the admission budget checks this before allocating).
+    static size_t required_bytes(size_t max_keys, size_t max_items, int threads, int sign_grid, int verify_grid) {
+        return max_keys * (align256(C::SK_ROW) + align256(C::PK_ROW)) + max_items * (C::ITEM_BYTES + 2 * sizeof(unsigned)) +
+               stage_bytes(max_items) + sizeof(FusedQueue) +
+               std::max((size_t)sign_grid * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
+    }
+
+    template <int T>
+    int configure() {
+        sign_smem = FusedSignSmem<MODE, T>::BYTES;
+        verify_smem = FusedVerifySmem<MODE, T>::BYTES;
+        if (cudaFuncSetAttribute(k_fused_sign<MODE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sign_smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_fused_verify<MODE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)verify_smem) != cudaSuccess)
+            return CUDIL_ERR_CUDA;
+        sign_grid = grid_for<T>((const void *)k_fused_sign<MODE, T>, sign_smem, sm_count);
+        verify_grid = grid_for<T>((const void *)k_fused_verify<MODE, T>, verify_smem, sm_count);
+        return (sign_grid > 0 && verify_grid > 0) ? CUDIL_OK : CUDIL_ERR_CUDA;
+    }
+
+    int create(size_t mk, size_t mi, int thr, size_t budget) {
+        mode = MODE;
+        max_keys = mk;
+        max_items = mi;
+        threads = thr;
+        if (mk == 0 || mi == 0 || mi > (1u << 24)) return CUDIL_ERR_INVALID;
+        if (cudaGetDevice(&device) != cudaSuccess) return CUDIL_ERR_CUDA;
+        if (cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return CUDIL_ERR_CUDA;
+        int rc = (threads == 128) ? configure<128>() : (threads == 256 ? configure<256>() : CUDIL_ERR_INVALID);
+        if (rc) return rc;
+        prehash_grid = (int)std::min<size_t>((mi + kBlock - 1) / kBlock, (size_t)sm_count * 8);
+        device_bytes = required_bytes(mk, mi, threads, sign_grid, verify_grid);
+        if (budget && device_bytes > budget) return CUDIL_ERR_BUDGET;
+        sk_pitch = align256(C::SK_ROW);
+        pk_pitch = align256(C::PK_ROW);
+        scratch_bytes = std::max((size_t)sign_grid * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
+        if (cudaMalloc(&sk_cache, mk * sk_pitch) != cudaSuccess || cudaMalloc(&pk_cache, mk * pk_pitch) != cudaSuccess ||
+            cudaMalloc(&items, mi * C::ITEM_BYTES) != cudaSuccess || cudaMalloc(&best, mi * sizeof(unsigned)) != cudaSuccess ||
+            cudaMalloc(&locks, mi * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&q, sizeof(FusedQueue)) != cudaSuccess ||
+            cudaMalloc(&d_key, mi * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&d_mlen, mi * sizeof(unsigned)) != cudaSuccess ||
+            cudaMalloc(&d_order, mi * sizeof(unsigned)) != cudaSuccess ||
+            cudaMalloc(&d_off, mi * sizeof(unsigned long long)) != cudaSuccess || cudaMalloc(&scratch, scratch_bytes) != cudaSuccess ||
+            cudaMallocHost(&h_stage, stage_bytes(mi)) != cudaSuccess || cudaMallocHost(&h_status, sizeof(FusedQueue)) != cudaSuccess)
+            return CUDIL_ERR_CUDA;
+        std::memset(h_status, 0, sizeof(FusedQueue));
+        return cudaMemset(q, 0, sizeof(FusedQueue)) == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
+    }
+
+    ~EngineImpl() override {
+        if (g_sign) cudaGraphExecDestroy(g_sign);
+        if (g_verify) cudaGraphExecDestroy(g_verify);
+        cudaFree(sk_cache);
+        cudaFree(pk_cache);
+        cudaFree(items);
+        cudaFree(best);
+        cudaFree(locks);
+        cudaFree(q);
+        cudaFree(d_key);
+        cudaFree(d_mlen);
+        cudaFree(d_order);
+        cudaFree(d_off);
+        cudaFree(scratch);
+        if (h_stage) cudaFreeHost(h_stage);
+        if (h_status) cudaFreeHost(h_status);
+    }
+
+    // ------------------------------------------------------------ key caches
+    int set_secret_keys(const uint8_t *d_sk, size_t nkeys, cudaStream_t st) {
+        if (!d_sk || nkeys == 0 || nkeys > max_keys) return CUDIL_ERR_INVALID;
+        const int nn = (int)nkeys;
+        CUDIL_LAUNCH(KID_CACHE_SK, st,
+                     k_cache_sk<MODE><<<blocks_for(nkeys * (PM::L + 2 * PM::K + 1) * 16), kBlock, 0, st>>>(d_sk, sk_cache, sk_pitch, nn));
+        CUDIL_CK_LAUNCH();
+        CUDIL_LAUNCH(KID_EXPAND_A, st,
+                     k_expand_a<MODE><<<blocks_for(nkeys * PM::K * PM::L), kBlock, 0, st>>>(sk_cache, sk_pitch, C::SK_RHO, C::SK_MAT, nn));
+        CUDIL_CK_LAUNCH();
+        n_sk = nkeys;
+        return CUDIL_OK;
+    }
+
+    int set_public_keys(const uint8_t *d_pk, size_t nkeys, cudaStream_t st) {
+        if (!d_pk || nkeys == 0 || nkeys > max_keys) return CUDIL_ERR_INVALID;
+        const int nn = (int)nkeys;
+        CUDIL_LAUNCH(KID_CACHE_PK, st, k_cache_pk_tr<MODE><<<blocks_for(nkeys), kBlock, 0, st>>>(d_pk, pk_cache, pk_pitch, nn));
+        CUDIL_CK_LAUNCH();
+        CUDIL_LAUNCH(KID_CACHE_PK, st,
+                     k_cache_pk_t1<MODE><<<blocks_for(nkeys * PM::K * 16), kBlock, 0, st>>>(d_pk, pk_cache, pk_pitch, nn));
+        CUDIL_CK_LAUNCH();
+        CUDIL_LAUNCH(KID_EXPAND_A, st,
+                     k_expand_a<MODE><<<blocks_for(nkeys * PM::K * PM::L), kBlock, 0, st>>>(pk_cache, pk_pitch, C::PK_RHO, C::PK_MAT, nn));
+        CUDIL_CK_LAUNCH();
+        n_pk = nkeys;
+        return CUDIL_OK;
+    }
+
+    // ------------------------------------------------------------ metadata upload
+    int upload_meta(const unsigned long long *off, const unsigned *mlen, const unsigned *key, size_t n, size_t nkeys,
+                    size_t msgs_bytes, bool longest_first, cudaStream_t st) {
+        // the previous batch's upload from the staging buffer must have completed
+        if (cudaStreamSynchronize(st) != cudaSuccess) return CUDIL_ERR_CUDA;
+        FusedQueue *hq = reinterpret_cast<FusedQueue *>(h_stage);
+        std::memset(hq, 0, sizeof(FusedQueue));
+        hq->n = (unsigned)n;
+        unsigned *hk = reinterpret_cast<unsigned *>(h_stage + 64);
+        unsigned *hm = hk + max_items;
+        unsigned *ho = hm + max_items;
+        unsigned long long *hoff = reinterpret_cast<unsigned long long *>(ho + max_items);
+        for (size_t i = 0; i < n; ++i) {
+            if (key[i] >= nkeys || (off[i] & 7u) || off[i] > msgs_bytes || mlen[i] > msgs_bytes - off[i])
+                return CUDIL_ERR_INVALID;
+            hk[i] = key[i];
+            hm[i] = mlen[i];
+            hoff[i] = off[i];
+        }
+        std::iota(ho, ho + n, 0u);
+        if (longest_first)
+            std::stable_sort(ho, ho + n, [&](unsigned a, unsigned b) { return hm[a] > hm[b]; });
+        CUDIL_CK(cudaMemcpyAsync(q, hq, sizeof(FusedQueue), cudaMemcpyHostToDevice, st));
+        CUDIL_CK(cudaMemcpyAsync(d_key, hk, n * sizeof(unsigned), cudaMemcpyHostToDevice, st));
+        CUDIL_CK(cudaMemcpyAsync(d_mlen, hm, n * sizeof(unsigned), cudaMemcpyHostToDevice, st));
+        CUDIL_CK(cudaMemcpyAsync(d_order, ho, n * sizeof(unsigned), cudaMemcpyHostToDevice, st));
+        CUDIL_CK(cudaMemcpyAsync(d_off, hoff, n * sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+        return CUDIL_OK;
+    }
+
+    // ------------------------------------------------------------ graphs
+    template <int T>
+    void record_sign(cudaStream_t st, uint8_t *d_sig, const uint8_t *d_msgs) {
+        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order};
+        k_fused_init<<<std::max(1, sm_count * 2), 256, 0, st>>>(q, best, locks);
+        k_fused_prehash<MODE><<<prehash_grid, kBlock, 0, st>>>(sk_cache, sk_pitch, mr, items, q);
+        k_fused_sign<MODE, T><<<sign_grid, T, sign_smem, st>>>(sk_cache, sk_pitch, d_key, items, d_sig, PM::SIG_BYTES, scratch, q,
+                                                              best, locks);
+        cudaMemcpyAsync(h_status, q, sizeof(FusedQueue), cudaMemcpyDeviceToHost, st);
+    }
+
+    template <int T>
+    void record_verify(cudaStream_t st, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs) {
+        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order};
+        k_fused_init<<<1, 32, 0, st>>>(q, best, locks);
+        k_fused_verify<MODE, T><<<verify_grid, T, verify_smem, st>>>(pk_cache, pk_pitch, mr, d_sig, PM::SIG_BYTES, d_ret,
+                                                                    scratch, q);
+        cudaMemcpyAsync(h_status, q, sizeof(FusedQueue), cudaMemcpyDeviceToHost, st);
+    }
+
+    int capture(cudaStream_t st, cudaGraphExec_t *exec, bool sign, uint8_t *out, const uint8_t *sig, const uint8_t *msgs) {
+        // graphs are captured on a private stream and launched on the caller's stream
+        cudaStream_t cs;
+        CUDIL_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t graph;
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            if (sign)
+                (threads == 128) ? record_sign<128>(cs, out, msgs) : record_sign<256>(cs, out, msgs);
+            else
+                (threads == 128) ? record_verify<128>(cs, reinterpret_cast<int *>(out), sig, msgs)
+                                 : record_verify<256>(cs, reinterpret_cast<int *>(out), sig, msgs);
+            e = cudaStreamEndCapture(cs, &graph);
+        }
+        cudaStreamDestroy(cs);
+        (void)st;
+        if (e != cudaSuccess) return CUDIL_ERR_CUDA;
+        if (*exec) cudaGraphExecDestroy(*exec);
+        e = cudaGraphInstantiate(exec, graph, 0);
+        cudaGraphDestroy(graph);
+        return e == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
+    }
+
+    int sign(uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes, const unsigned long long *off, const unsigned *mlen,
+             const unsigned *key, size_t n, cudaStream_t st) {
+        if (n == 0) return CUDIL_OK;
+        if (!d_sig || !off || !mlen || !key || n > max_items || n_sk == 0) return CUDIL_ERR_INVALID;
+        if (!d_msgs) {
+            for (size_t i = 0; i < n; ++i)
+                if (mlen[i]) return CUDIL_ERR_INVALID;
+            d_msgs = reinterpret_cast<const uint8_t *>(items);  // any aligned pointer; never read
+        }
+        if (((uintptr_t)d_msgs) & 7u) return CUDIL_ERR_INVALID;
+        int rc = upload_meta(off, mlen, key, n, n_sk, msgs_bytes, true, st);
+        if (rc) return rc;
+        if (!g_sign || g_sign_key[0] != d_sig || g_sign_key[1] != d_msgs) {
+            rc = capture(st, &g_sign, true, d_sig, nullptr, d_msgs);
+            if (rc) return rc;
+            g_sign_key[0] = d_sig;
+            g_sign_key[1] = d_msgs;
+        }
+        CUDIL_LAUNCH(KID_FUSED_SIGN, st, cudaGraphLaunch(g_sign, st));
+        CUDIL_CK_LAUNCH();
+        Profiler::get().launches.fetch_add(2);  // the graph holds init + prehash + sign kernels
+        return CUDIL_OK;
+    }
+
+    int verify(int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes, const unsigned long long *off,
+               const unsigned *mlen, const unsigned *key, size_t n, cudaStream_t st) {
+        if (n == 0) return CUDIL_OK;
+        if (!d_ret || !d_sig || !off || !mlen || !key || n > max_items || n_pk == 0) return CUDIL_ERR_INVALID;
+        if (!d_msgs) {
+            for (size_t i = 0; i < n; ++i)
+                if (mlen[i]) return CUDIL_ERR_INVALID;
+            d_msgs = reinterpret_cast<const uint8_t *>(items);
+        }
+        if (((uintptr_t)d_msgs) & 7u) return CUDIL_ERR_INVALID;
+        int rc = upload_meta(off, mlen, key, n, n_pk, msgs_bytes, false, st);
+        if (rc) return rc;
+        if (!g_verify || g_verify_key[0] != d_ret || g_verify_key[1] != d_sig || d_msgs != g_verify_msgs) {
+            rc = capture(st, &g_verify, false, reinterpret_cast<uint8_t *>(d_ret), d_sig, d_msgs);
+            if (rc) return rc;
+            g_verify_key[0] = d_ret;
+            g_verify_key[1] = d_sig;
+            g_verify_msgs = d_msgs;
+        }
+        CUDIL_LAUNCH(KID_FUSED_VERIFY, st, cudaGraphLaunch(g_verify, st));
+        CUDIL_CK_LAUNCH();
+        Profiler::get().launches.fetch_add(1);  // the graph holds init + verify kernels
+        return CUDIL_OK;
+    }
+
+    const uint8_t *g_verify_msgs = nullptr;
+};
+
+}  // namespace cudil

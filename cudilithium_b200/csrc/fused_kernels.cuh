@@ -1,0 +1,744 @@
+// Fused / persistent form of the batched path (no reference counterpart; the reference drives
+// every rejection round from the host, src/api.cu:218-441).
+//
+//  * Per-key resident cache (built once per key, reused by every message of that key):
+//      secret rows  [rho | K | tr | pad..256 | A_hat (K*L polys) | s1_hat | s2_hat | t0_hat]
+//      public rows  [rho | tr | pad..256 | A_hat (K*L polys) | t1_hat = NTT(t1 * 2^d)]
+//  * k_fused_prehash  one thread per message, longest messages first: mu = H(tr||m), rho' = H(K||mu)
+//  * k_fused_sign     ONE persistent kernel for all signing attempts of a batch.  A device ticket
+//                     queue hands out (item, nonce) attempts -- ticket t is (t mod n, t div n), so the
+//                     nonces of every item are issued in increasing order -- and skips attempts whose
+//                     item already has an accepted smaller nonce.  Each block claims up to A live
+//                     attempts, runs ExpandMask (thread per attempt), w = A*y (16-thread group per
+//                     attempt), challenge (thread per attempt), rejection checks + hints (group per
+//                     attempt) and refills its slots from the queue.  An accepted attempt lowers the
+//                     item's best nonce with atomicMin and, under a per-item lock with a bounded spin,
+//                     publishes its signature only if it still holds the minimum -- the same
+//                     smallest-accepted-nonce result as deterministic signing (src/api.cu:388-411).
+//  * k_fused_verify   persistent verification against public rows (no ExpandA / H(pk) per signature).
+#pragma once
+
+#include "keypair_kernels.cuh"
+#include "verify_kernels.cuh"
+
+namespace cudil {
+
+template <int MODE>
+struct Cache {
+    using PM = P<MODE>;
+    static constexpr int K = PM::K, L = PM::L;
+    static constexpr size_t POLY = N * sizeof(int32_t);
+    // secret-key rows
+    static constexpr size_t SK_RHO = 0, SK_KEY = 32, SK_TR = 64;
+    static constexpr size_t SK_MAT = 256;
+    static constexpr size_t SK_S1 = SK_MAT + (size_t)K * L * POLY;
+    static constexpr size_t SK_S2 = SK_S1 + (size_t)L * POLY;
+    static constexpr size_t SK_T0 = SK_S2 + (size_t)K * POLY;
+    static constexpr size_t SK_ROW = SK_T0 + (size_t)K * POLY;
+    // public-key rows
+    static constexpr size_t PK_RHO = 0, PK_TR = 32;
+    static constexpr size_t PK_MAT = 256;
+    static constexpr size_t PK_T1 = PK_MAT + (size_t)K * L * POLY;
+    static constexpr size_t PK_ROW = PK_T1 + (size_t)K * POLY;
+    // per-message prologue output: mu | rho'
+    static constexpr size_t ITEM_BYTES = 128;
+    // per-attempt slot of the persistent signer
+    static constexpr size_t SL_Y = 0;
+    static constexpr size_t SL_W0 = align256((size_t)L * PM::POLYZ_PACKED);
+    static constexpr size_t SL_W1P = SL_W0 + (size_t)K * POLY;
+    static constexpr size_t SL_CM = SL_W1P + align256(PM::W1PACKED_BYTES);
+    static constexpr size_t SL_SIG = SL_CM + 256;
+    static constexpr size_t SLOT = SL_SIG + align256(PM::SIG_BYTES);
+    // per-signature slot of the persistent verifier: mu | w1' | c masks | status
+    static constexpr size_t VS_MU = 0;
+    static constexpr size_t VS_W1 = 64;
+    static constexpr size_t VS_CM = align256(64 + PM::W1PACKED_BYTES);
+    static constexpr size_t VS_STATUS = VS_CM + 64;
+    static constexpr size_t VSLOT = VS_CM + 256;
+};
+
+// Queue / status block shared by the engine kernels (one per engine, device memory).
+struct FusedQueue {
+    unsigned long long next_ticket;
+    unsigned int done_items;
+    unsigned int error;        // bit 0: a bounded lock wait gave up
+    unsigned long long attempts;
+    unsigned int n;            // items in the current batch
+    unsigned int pad;
+};
+
+// ------------------------------------------------------------------ cache builders
+
+// Secret rows from packed secret keys (dense, SK_BYTES each): rho, K, tr copied; s1, s2, t0
+// unpacked and transformed.  One group per polynomial (+ group p == L+2K copies the seeds).
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_cache_sk(const uint8_t *sk, uint8_t *rows, size_t pitch, int n) {
+    using PM = P<MODE>;
+    using C = Cache<MODE>;
+    constexpr int K = PM::K, L = PM::L, NP = L + 2 * K + 1;
+    __shared__ int32_t sm[kGroupsPerBlock * NTT_SMEM_WORDS];
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const int it = gid / NP, p = gid % NP;
+    if (it >= n) return;
+    Group g = make_group(sm, threadIdx.x >> 4);
+    const uint8_t *s = sk + (size_t)it * PM::SK_BYTES;
+    uint8_t *row = rows + (size_t)it * pitch;
+    if (p == NP - 1) {
+        // rho | K | tr are the first 96 bytes of sk
+        for (int b = g.t; b < 96; b += 16) row[b] = s[b];
+        return;
+    }
+    int32_t x[16];
+    size_t dst;
+    if (p < L + K) {
+        const uint8_t *src = s + PM::SK_S1 + (size_t)p * PM::POLYETA_PACKED;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) x[i] = PM::ETA - (int32_t)get_bits(src, (g.t + 16 * i) * PM::ETA_BITS, PM::ETA_BITS);
+        dst = (p < L) ? C::SK_S1 + (size_t)p * C::POLY : C::SK_S2 + (size_t)(p - L) * C::POLY;
+    } else {
+        const uint8_t *src = s + PM::SK_T0 + (size_t)(p - L - K) * POLYT0_PACKED;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            // last coefficient of the last t0 poly ends exactly at SK_BYTES: read 2 bytes only
+            const int bit = (g.t + 16 * i) * 13, byte = bit >> 3, sh = bit & 7;
+            const uint32_t v = ((uint32_t)src[byte] | ((uint32_t)src[byte + 1] << 8) |
+                                (sh + 13 > 16 ? (uint32_t)src[byte + 2] << 16 : 0u)) >> sh;
+            x[i] = (1 << (D - 1)) - (int32_t)(v & 0x1FFFu);
+        }
+        dst = C::SK_T0 + (size_t)(p - L - K) * C::POLY;
+    }
+    ntt16(x, g.sm, g.gmask, g.t);
+    store16_contig(reinterpret_cast<int32_t *>(row + dst) + 16 * g.t, x);
+}
+
+// Public rows: tr = H(pk) and rho (thread per key) ...
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_cache_pk_tr(const uint8_t *pk, uint8_t *rows, size_t pitch, int n) {
+    using PM = P<MODE>;
+    using C = Cache<MODE>;
+    const int it = blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= n) return;
+    const uint8_t *p = pk + (size_t)it * PM::PK_BYTES;
+    uint8_t *row = rows + (size_t)it * pitch;
+    uint32_t al[25], ah[25];
+    // pk rows of a dense array are only 4-byte aligned when PK_BYTES % 8 != 0: read bytewise
+    struct Src {
+        const uint8_t *p;
+        __device__ uint2 lane(long long g) const { return load_lane_bytes(p + g * 8, (int)(PM::PK_BYTES - g * 8)); }
+    } src{p};
+    shake_absorb<SHAKE256_RATE>(al, ah, src, PM::PK_BYTES);
+    keccak_f1600(al, ah);
+    uint2 *tr = reinterpret_cast<uint2 *>(row + C::PK_TR);
+#pragma unroll
+    for (int w = 0; w < 4; ++w) tr[w] = make_uint2(al[w], ah[w]);
+    for (int b = 0; b < 32; ++b) row[C::PK_RHO + b] = p[b];
+}
+
+// ... and t1_hat = NTT(t1 * 2^d) (group per polynomial).
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_cache_pk_t1(const uint8_t *pk, uint8_t *rows, size_t pitch, int n) {
+    using PM = P<MODE>;
+    using C = Cache<MODE>;
+    constexpr int K = PM::K;
+    __shared__ int32_t sm[kGroupsPerBlock * NTT_SMEM_WORDS];
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const int it = gid / K, i = gid % K;
+    if (it >= n) return;
+    Group g = make_group(sm, threadIdx.x >> 4);
+    const uint8_t *t1p = pk + (size_t)it * PM::PK_BYTES + SEEDBYTES + (size_t)i * POLYT1_PACKED;
+    int32_t x[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int bit = (g.t + 16 * m) * 10, byte = bit >> 3, sh = bit & 7;
+        const uint32_t v = ((uint32_t)t1p[byte] | ((uint32_t)t1p[byte + 1] << 8)) >> sh;  // sh + 10 <= 16
+        x[m] = (int32_t)((v & 0x3FFu) << D);
+    }
+    ntt16(x, g.sm, g.gmask, g.t);
+    store16_contig(reinterpret_cast<int32_t *>(rows + (size_t)it * pitch + C::PK_T1 + (size_t)i * C::POLY) + 16 * g.t, x);
+}
+
+// ------------------------------------------------------------------ per-batch prologue
+
+// Messages live in one device buffer at 8-byte aligned offsets.  order[] lists the items longest
+// first so a warp's messages have similar lengths.
+struct MsgRefs {
+    const uint8_t *msgs;
+    const unsigned long long *offsets;
+    const unsigned int *mlens;
+    const unsigned int *key_idx;
+    const unsigned int *order;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_fused_prehash(const uint8_t *cache, size_t cpitch, MsgRefs mr, uint8_t *items,
+                                                          const FusedQueue *q) {
+    using C = Cache<MODE>;
+    const unsigned n = q->n;
+    for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const unsigned it = mr.order[r];
+        const uint8_t *row = cache + (size_t)mr.key_idx[it] * cpitch;
+        uint32_t al[25], ah[25];
+        TwoPart src{row + C::SK_TR, 4, mr.msgs + mr.offsets[it], (long long)mr.mlens[it]};
+        shake_absorb<SHAKE256_RATE>(al, ah, src, (long long)SEEDBYTES + mr.mlens[it]);
+        keccak_f1600(al, ah);
+        uint2 mu[8];
+#pragma unroll
+        for (int w = 0; w < 8; ++w) mu[w] = make_uint2(al[w], ah[w]);
+        uint2 *out = reinterpret_cast<uint2 *>(items + (size_t)it * C::ITEM_BYTES);
+#pragma unroll
+        for (int w = 0; w < 8; ++w) out[w] = mu[w];
+        uint2 key[4];
+        ld_lanes(key, row + C::SK_KEY);
+        keccak_zero(al, ah);
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            al[w] = key[w].x;
+            ah[w] = key[w].y;
+        }
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            al[4 + w] = mu[w].x;
+            ah[4 + w] = mu[w].y;
+        }
+        al[12] ^= 0x1Fu;
+        ah[16] ^= 0x80000000u;
+        keccak_f1600(al, ah);
+#pragma unroll
+        for (int w = 0; w < 8; ++w) out[8 + w] = make_uint2(al[w], ah[w]);
+    }
+}
+
+// Resets the per-item winner state and the queue for q->n items (n set by the host copy).
+static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *locks) {
+    const unsigned n = q->n;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        best[i] = 0xFFFFFFFFu;
+        locks[i] = 0u;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        q->next_ticket = 0;
+        q->done_items = 0;
+        q->error = 0;
+        q->attempts = 0;
+    }
+}
+
+// ------------------------------------------------------------------ persistent signer
+
+template <int MODE, int THREADS>
+struct FusedSignSmem {
+    using PM = P<MODE>;
+    static constexpr int G = THREADS / 16;
+    static constexpr size_t CTRL = 4096;
+    static constexpr size_t PH_W = (size_t)G * (PM::L * N * 4 + NTT_SMEM_WORDS * 4);
+    static constexpr size_t PH_C = (size_t)THREADS * (SHAKE256_RATE + 64);
+    static constexpr size_t BYTES = CTRL + (PH_W > PH_C ? PH_W : PH_C);
+};
+
+constexpr unsigned kLockSpinLimit = 1u << 22;
+
+template <int MODE, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_fused_sign(const uint8_t *cache, size_t cpitch, const unsigned *key_idx,
+                                                        const uint8_t *items, uint8_t *sig_out, size_t sig_pitch,
+                                                        uint8_t *scratch, FusedQueue *q, unsigned *best,
+                                                        unsigned *locks) {
+    using PM = P<MODE>;
+    using C = Cache<MODE>;
+    constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA, A = THREADS;
+    constexpr int G = THREADS / 16;
+    extern __shared__ __align__(16) uint8_t fs_smem[];
+    unsigned *s_item = reinterpret_cast<unsigned *>(fs_smem);          // [A]
+    unsigned *s_nonce = s_item + A;                                      // [A]
+    unsigned *s_ctl = s_nonce + A;                                       // [8]
+    uint8_t *ph = fs_smem + FusedSignSmem<MODE, THREADS>::CTRL;         // phase-shared region
+    const int tid = threadIdx.x, gi = tid >> 4, lane = tid & 31;
+    const unsigned n = q->n;
+    const unsigned long long total = (unsigned long long)n * 65536ull;  // nonce is 16-bit
+    uint8_t *my_slots = scratch + (size_t)blockIdx.x * A * C::SLOT;
+
+    for (;;) {
+        // ---------------- claim up to A live attempts from the ticket queue
+        if (tid == 0) s_ctl[0] = 0;  // filled
+        __syncthreads();
+        for (;;) {
+            if (tid == 0) {
+                const unsigned filled = s_ctl[0];
+                const unsigned done = *reinterpret_cast<volatile unsigned *>(&q->done_items);
+                unsigned need = (done >= n) ? 0u : (unsigned)A - filled;
+                unsigned long long base = 0;
+                if (need) {
+                    base = atomicAdd(&q->next_ticket, (unsigned long long)need);
+                    if (base >= total) need = 0;
+                }
+                s_ctl[1] = need;
+                s_ctl[2] = (unsigned)(base & 0xFFFFFFFFull);
+                s_ctl[3] = (unsigned)(base >> 32);
+            }
+            __syncthreads();
+            const unsigned need = s_ctl[1];
+            if (need == 0) break;
+            const unsigned long long t = ((unsigned long long)s_ctl[3] << 32 | s_ctl[2]) + (unsigned)tid;
+            bool live = false;
+            unsigned item = 0, nonce = 0;
+            if ((unsigned)tid < need && t < total) {
+                item = (unsigned)(t % n);
+                nonce = (unsigned)(t / n);
+                live = __ldcg(best + item) > nonce;
+            }
+            // block-wide compaction of the live tickets into the slot list
+            const unsigned bal = __ballot_sync(0xFFFFFFFFu, live);
+            if (lane == 0) s_ctl[4 + 0] = 0;  // placeholder (warp offsets computed below)
+            __shared__ unsigned s_wcnt[THREADS / 32];
+            if (lane == 0) s_wcnt[tid >> 5] = __popc(bal);
+            __syncthreads();
+            unsigned off = s_ctl[0];
+            for (int w = 0; w < (tid >> 5); ++w) off += s_wcnt[w];
+            if (live) {
+                const unsigned pos = off + __popc(bal & ((1u << lane) - 1u));
+                s_item[pos] = item;
+                s_nonce[pos] = nonce;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                unsigned tot = 0;
+                for (int w = 0; w < THREADS / 32; ++w) tot += s_wcnt[w];
+                s_ctl[0] += tot;
+            }
+            __syncthreads();
+            if (s_ctl[0] >= (unsigned)A) break;
+        }
+        const int na = (int)s_ctl[0];
+        if (na == 0) break;
+        if (tid == 0) atomicAdd(&q->attempts, (unsigned long long)na);
+
+        // ---------------- ExpandMask: one thread per attempt, L streams each
+        if (tid < na) {
+            const unsigned item = s_item[tid], nonce = s_nonce[tid];
+            uint2 rhop[8];
+            ld_lanes(rhop, items + (size_t)item * C::ITEM_BYTES + 64);
+            uint8_t *slot = my_slots + (size_t)tid * C::SLOT;
+#pragma unroll 1
+            for (int j = 0; j < L; ++j)
+                expand_mask_stream<MODE>(slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, rhop, (uint32_t)(L * nonce + j));
+        }
+        __syncthreads();
+
+        // ---------------- w = invNTT(A_hat * NTT(y)), Decompose: one group per attempt
+        {
+            int32_t *yh = reinterpret_cast<int32_t *>(ph) + (size_t)gi * (L * N + NTT_SMEM_WORDS);
+            Group g;
+            g.t = tid & 15;
+            g.gmask = 0xFFFFu << (lane & 16);
+            g.sm = yh + L * N;
+            for (int a = gi; a < na; a += G) {
+                uint8_t *slot = my_slots + (size_t)a * C::SLOT;
+                const uint8_t *row = cache + (size_t)key_idx[s_item[a]] * cpitch;
+#pragma unroll 1
+                for (int j = 0; j < L; ++j) {
+                    int32_t x[16];
+                    unpack_z_strided<MODE>(x, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
+                    ntt16(x, g.sm, g.gmask, g.t);
+                    store16_contig(yh + j * N + 16 * g.t, x);
+                }
+                __syncwarp(g.gmask);
+#pragma unroll 1
+                for (int i = 0; i < K; ++i) {
+                    const int32_t *mat = reinterpret_cast<const int32_t *>(row + C::SK_MAT) + (size_t)i * L * N;
+                    int32_t acc[16];
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) acc[m] = 0;
+#pragma unroll
+                    for (int j = 0; j < L; ++j) {
+                        int32_t av[16], yv[16];
+                        load16_contig(av, mat + (size_t)j * N + 16 * g.t);
+                        load16_contig(yv, yh + j * N + 16 * g.t);
+#pragma unroll
+                        for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], yv[m]);
+                    }
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m]);
+                    intt16(acc, g.sm, g.gmask, g.t);
+                    int32_t *w0 = reinterpret_cast<int32_t *>(slot + C::SL_W0) + (size_t)i * N;
+                    int32_t w1[16];
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) {
+                        int32_t a0;
+                        w1[m] = decompose<MODE>(a0, caddq(acc[m]));
+                        w0[g.t + 16 * m] = a0;
+                    }
+                    int32_t w1c[16];
+                    strided_to_contig(g, w1, w1c);
+                    uint32_t v[16];
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) v[m] = (uint32_t)w1c[m];
+                    pack16_words<PM::W1_BITS>(
+                        reinterpret_cast<uint32_t *>(slot + C::SL_W1P + (size_t)i * PM::POLYW1_PACKED + g.t * 2 * PM::W1_BITS), v);
+                }
+                __syncwarp(g.gmask);
+            }
+        }
+        __syncthreads();
+
+        // ---------------- challenge: one thread per attempt
+        if (tid < na) {
+            const unsigned item = s_item[tid];
+            uint8_t *slot = my_slots + (size_t)tid * C::SLOT;
+            uint32_t al[25], ah[25];
+            TwoPart src{items + (size_t)item * C::ITEM_BYTES, 8, slot + C::SL_W1P, PM::W1PACKED_BYTES};
+            shake_absorb<SHAKE256_RATE>(al, ah, src, CRHBYTES + PM::W1PACKED_BYTES);
+            keccak_f1600(al, ah);
+            uint2 ct[4];
+#pragma unroll
+            for (int w = 0; w < 4; ++w) ct[w] = make_uint2(al[w], ah[w]);
+            uint2 *sg = reinterpret_cast<uint2 *>(slot + C::SL_SIG);
+#pragma unroll
+            for (int w = 0; w < 4; ++w) sg[w] = ct[w];
+            uint8_t *blk = ph + (size_t)tid * SHAKE256_RATE;
+            uint32_t *mask = reinterpret_cast<uint32_t *>(ph + (size_t)THREADS * SHAKE256_RATE) + tid * 16;
+            sample_in_ball<PM::TAU>(ct, blk, mask);
+            uint4 *mo = reinterpret_cast<uint4 *>(slot + C::SL_CM);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) mo[k] = make_uint4(mask[4 * k], mask[4 * k + 1], mask[4 * k + 2], mask[4 * k + 3]);
+        }
+        __syncthreads();
+
+        // ---------------- rejection checks, hints, publication: one group per attempt
+        {
+            Group g;
+            g.t = tid & 15;
+            g.gmask = 0xFFFFu << (lane & 16);
+            g.sm = reinterpret_cast<int32_t *>(ph) + (size_t)gi * NTT_SMEM_WORDS;
+            const int lane_off = lane & 16;
+            for (int a = gi; a < na; a += G) {
+                const unsigned item = s_item[a], nonce = s_nonce[a];
+                uint8_t *slot = my_slots + (size_t)a * C::SLOT;
+                const uint8_t *row = cache + (size_t)key_idx[item] * cpitch;
+                uint32_t masks[16];
+                {
+                    const uint4 *mi = reinterpret_cast<const uint4 *>(slot + C::SL_CM);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const uint4 v = mi[k];
+                        masks[4 * k] = v.x;
+                        masks[4 * k + 1] = v.y;
+                        masks[4 * k + 2] = v.z;
+                        masks[4 * k + 3] = v.w;
+                    }
+                }
+                int32_t ch[16];
+                challenge_strided(ch, masks, g.t);
+                ntt16(ch, g.sm, g.gmask, g.t);
+                bool rejected = false;
+                const int32_t *s1 = reinterpret_cast<const int32_t *>(row + C::SK_S1);
+#pragma unroll 1
+                for (int j = 0; j < L && !rejected; ++j) {
+                    int32_t x[16], y[16];
+                    load16_contig(x, s1 + (size_t)j * N + 16 * g.t);
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
+                    intt16(x, g.sm, g.gmask, g.t);
+                    unpack_z_strided<MODE>(y, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
+                    bool bad = false;
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) {
+                        x[m] = reduce32(x[m] + y[m]);
+                        bad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
+                    }
+                    if (group_any(g, bad)) {
+                        rejected = true;
+                        break;
+                    }
+                    int32_t zc[16];
+                    strided_to_contig(g, x, zc);
+                    uint32_t v[16];
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
+                    pack16_words<PM::Z_BITS>(reinterpret_cast<uint32_t *>(slot + C::SL_SIG + PM::SIG_Z + (size_t)j * PM::POLYZ_PACKED +
+                                                                          g.t * 2 * PM::Z_BITS),
+                                             v);
+                }
+                if (rejected) continue;
+                const int32_t *s2 = reinterpret_cast<const int32_t *>(row + C::SK_S2);
+                const int32_t *t0 = reinterpret_cast<const int32_t *>(row + C::SK_T0);
+                uint8_t *hs = slot + C::SL_SIG + PM::SIG_H;
+                int cnt = 0;
+#pragma unroll 1
+                for (int i = 0; i < K && !rejected; ++i) {
+                    int32_t x[16], r0[16];
+                    load16_contig(x, s2 + (size_t)i * N + 16 * g.t);
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
+                    intt16(x, g.sm, g.gmask, g.t);
+                    const int32_t *w0 = reinterpret_cast<const int32_t *>(slot + C::SL_W0) + (size_t)i * N;
+                    bool bad = false;
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) {
+                        r0[m] = reduce32(w0[g.t + 16 * m] - x[m]);
+                        bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
+                    }
+                    if (group_any(g, bad)) {
+                        rejected = true;
+                        break;
+                    }
+                    load16_contig(x, t0 + (size_t)i * N + 16 * g.t);
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
+                    intt16(x, g.sm, g.gmask, g.t);
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) {
+                        x[m] = reduce32(x[m]);
+                        bad |= exceeds(x[m], PM::GAMMA2);
+                    }
+                    if (group_any(g, bad)) {
+                        rejected = true;
+                        break;
+                    }
+                    const uint8_t *w1p = slot + C::SL_W1P + (size_t)i * PM::POLYW1_PACKED;
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) {
+                        const int32_t w1 = (int32_t)get_bits(w1p, (g.t + 16 * m) * PM::W1_BITS, PM::W1_BITS);
+                        const unsigned h = make_hint<MODE>(r0[m] + x[m], w1);
+                        const unsigned bal = (__ballot_sync(g.gmask, h) >> lane_off) & 0xFFFFu;
+                        if (h) {
+                            const int idx = cnt + __popc(bal & ((1u << g.t) - 1u));
+                            if (idx < OMEGA) hs[idx] = (uint8_t)(g.t + 16 * m);
+                        }
+                        cnt += __popc(bal);
+                    }
+                    if (cnt > OMEGA) {
+                        rejected = true;
+                        break;
+                    }
+                    if (g.t == 0) hs[OMEGA + i] = (uint8_t)cnt;
+                }
+                if (rejected) continue;
+                for (int qq = cnt + g.t; qq < OMEGA; qq += 16) hs[qq] = 0;
+                __syncwarp(g.gmask);
+                // accepted: lower the item's best nonce; publish if this attempt holds the minimum
+                unsigned old = 0;
+                if (g.t == 0) old = atomicMin(best + item, nonce);
+                old = __shfl_sync(g.gmask, old, lane_off);
+                if (nonce < old) {
+                    if (g.t == 0 && old == 0xFFFFFFFFu) atomicAdd(&q->done_items, 1u);
+                    int got = 0;
+                    if (g.t == 0) {
+                        for (unsigned spin = 0; spin < kLockSpinLimit; ++spin) {
+                            if (atomicCAS(locks + item, 0u, 1u) == 0u) {
+                                got = 1;
+                                break;
+                            }
+                            __nanosleep(64);
+                        }
+                        if (!got) atomicOr(&q->error, 1u);
+                    }
+                    got = __shfl_sync(g.gmask, got, lane_off);
+                    if (got) {
+                        __threadfence();
+                        unsigned cur = 0;
+                        if (g.t == 0) cur = *reinterpret_cast<volatile unsigned *>(best + item);
+                        cur = __shfl_sync(g.gmask, cur, lane_off);
+                        if (cur == nonce) {
+                            const uint8_t *src = slot + C::SL_SIG;
+                            uint8_t *dst = sig_out + (size_t)item * sig_pitch;
+                            for (int b = g.t; b < PM::SIG_BYTES; b += 16) dst[b] = src[b];
+                        }
+                        __threadfence();
+                        __syncwarp(g.gmask);
+                        if (g.t == 0) atomicExch(locks + item, 0u);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ persistent verifier
+
+template <int MODE, int THREADS>
+struct FusedVerifySmem {
+    using PM = P<MODE>;
+    static constexpr int G = THREADS / 16;
+    static constexpr size_t PH_W = (size_t)G * ((PM::L + 1) * N * 4 + NTT_SMEM_WORDS * 4 + 32);
+    static constexpr size_t PH_C = (size_t)THREADS * (SHAKE256_RATE + 64);
+    static constexpr size_t BYTES = 256 + (PH_W > PH_C ? PH_W : PH_C);
+};
+
+template <int MODE, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_fused_verify(const uint8_t *cache, size_t cpitch, MsgRefs mr,
+                                                          const uint8_t *sig, size_t sig_pitch, int *ret,
+                                                          uint8_t *scratch, FusedQueue *q) {
+    using PM = P<MODE>;
+    using C = Cache<MODE>;
+    constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA, A = THREADS, G = THREADS / 16;
+    extern __shared__ __align__(16) uint8_t fv_smem[];
+    unsigned *s_ctl = reinterpret_cast<unsigned *>(fv_smem);
+    uint8_t *ph = fv_smem + 256;
+    const int tid = threadIdx.x, gi = tid >> 4, lane = tid & 31;
+    const unsigned n = q->n;
+    uint8_t *my_slots = scratch + (size_t)blockIdx.x * A * C::VSLOT;
+    for (;;) {
+        if (tid == 0) s_ctl[0] = (unsigned)atomicAdd(&q->next_ticket, (unsigned long long)A);
+        __syncthreads();
+        const unsigned base = s_ctl[0];
+        if (base >= n) break;
+        const int na = (int)((n - base) < (unsigned)A ? (n - base) : (unsigned)A);
+
+        // hint encoding checks, mu = H(tr||m), c = SampleInBall(c~): thread per signature
+        if (tid < na) {
+            const unsigned it = base + tid;
+            const uint8_t *s = sig + (size_t)it * sig_pitch;
+            const uint8_t *row = cache + (size_t)mr.key_idx[it] * cpitch;
+            uint8_t *slot = my_slots + (size_t)tid * C::VSLOT;
+            int status = 0;
+            const uint8_t *h = s + PM::SIG_H;
+            int k = 0;
+            for (int i = 0; i < K && !status; ++i) {
+                const int end = h[OMEGA + i];
+                if (end < k || end > OMEGA) {
+                    status = 1;
+                    break;
+                }
+                for (int j = k + 1; j < end; ++j)
+                    if (h[j] <= h[j - 1]) status = 1;
+                k = end;
+            }
+            if (!status)
+                for (int j = k; j < OMEGA; ++j)
+                    if (h[j]) status = 1;
+            uint32_t al[25], ah[25];
+            TwoPart src{row + C::PK_TR, 4, mr.msgs + mr.offsets[it], (long long)mr.mlens[it]};
+            shake_absorb<SHAKE256_RATE>(al, ah, src, (long long)SEEDBYTES + mr.mlens[it]);
+            keccak_f1600(al, ah);
+            uint2 *mu = reinterpret_cast<uint2 *>(slot + C::VS_MU);
+#pragma unroll
+            for (int w = 0; w < 8; ++w) mu[w] = make_uint2(al[w], ah[w]);
+            uint2 ct[4];
+#pragma unroll
+            for (int w = 0; w < 4; ++w) ct[w] = make_uint2(load_lane_bytes(s + 8 * w, 8).x, load_lane_bytes(s + 8 * w, 8).y);
+            uint8_t *blk = ph + (size_t)tid * SHAKE256_RATE;
+            uint32_t *mask = reinterpret_cast<uint32_t *>(ph + (size_t)THREADS * SHAKE256_RATE) + tid * 16;
+            sample_in_ball<PM::TAU>(ct, blk, mask);
+            uint4 *mo = reinterpret_cast<uint4 *>(slot + C::VS_CM);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) mo[kk] = make_uint4(mask[4 * kk], mask[4 * kk + 1], mask[4 * kk + 2], mask[4 * kk + 3]);
+            reinterpret_cast<int *>(slot + C::VS_STATUS)[0] = status;
+        }
+        __syncthreads();
+
+        // z norm check + NTT(z), NTT(c), w' = A_hat z_hat - c_hat t1_hat, UseHint, pack: group per signature
+        {
+            int32_t *zh = reinterpret_cast<int32_t *>(ph) + (size_t)gi * ((L + 1) * N + NTT_SMEM_WORDS + 8);
+            uint32_t *hbits = reinterpret_cast<uint32_t *>(zh + (L + 1) * N + NTT_SMEM_WORDS);
+            Group g;
+            g.t = tid & 15;
+            g.gmask = 0xFFFFu << (lane & 16);
+            g.sm = zh + (L + 1) * N;
+            for (int a = gi; a < na; a += G) {
+                const unsigned it = base + a;
+                const uint8_t *s = sig + (size_t)it * sig_pitch;
+                const uint8_t *row = cache + (size_t)mr.key_idx[it] * cpitch;
+                uint8_t *slot = my_slots + (size_t)a * C::VSLOT;
+                bool zbad = false;
+#pragma unroll 1
+                for (int j = 0; j < L; ++j) {
+                    int32_t x[16];
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) {
+                        const int bit = (g.t + 16 * m) * PM::Z_BITS;
+                        const uint8_t *pz = s + PM::SIG_Z + (size_t)j * PM::POLYZ_PACKED + (bit >> 3);
+                        const uint32_t v = ((uint32_t)pz[0] | ((uint32_t)pz[1] << 8) | ((uint32_t)pz[2] << 16)) >> (bit & 7);
+                        x[m] = PM::GAMMA1 - (int32_t)(v & ((1u << PM::Z_BITS) - 1u));
+                        zbad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
+                    }
+                    ntt16(x, g.sm, g.gmask, g.t);
+                    store16_contig(zh + j * N + 16 * g.t, x);
+                }
+                if (group_any(g, zbad) && g.t == 0) reinterpret_cast<int *>(slot + C::VS_STATUS)[0] |= 2;
+                {
+                    uint32_t masks[16];
+                    const uint4 *mi = reinterpret_cast<const uint4 *>(slot + C::VS_CM);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const uint4 v = mi[kk];
+                        masks[4 * kk] = v.x;
+                        masks[4 * kk + 1] = v.y;
+                        masks[4 * kk + 2] = v.z;
+                        masks[4 * kk + 3] = v.w;
+                    }
+                    int32_t x[16];
+                    challenge_strided(x, masks, g.t);
+                    ntt16(x, g.sm, g.gmask, g.t);
+                    store16_contig(zh + L * N + 16 * g.t, x);
+                }
+                __syncwarp(g.gmask);
+                const uint8_t *h = s + PM::SIG_H;
+#pragma unroll 1
+                for (int i = 0; i < K; ++i) {
+                    if (g.t < 8) hbits[g.t] = 0;
+                    __syncwarp(g.gmask);
+                    const int start = (i == 0) ? 0 : h[OMEGA + i - 1];
+                    int end = h[OMEGA + i];
+                    if (end > OMEGA) end = OMEGA;
+                    for (int j = start + g.t; j < end; j += 16) atomicOr(&hbits[h[j] >> 5], 1u << (h[j] & 31));
+                    __syncwarp(g.gmask);
+                    const int32_t *mat = reinterpret_cast<const int32_t *>(row + C::PK_MAT) + (size_t)i * L * N;
+                    int32_t acc[16];
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) acc[m] = 0;
+#pragma unroll
+                    for (int j = 0; j < L; ++j) {
+                        int32_t av[16], zv[16];
+                        load16_contig(av, mat + (size_t)j * N + 16 * g.t);
+                        load16_contig(zv, zh + j * N + 16 * g.t);
+#pragma unroll
+                        for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], zv[m]);
+                    }
+                    int32_t cv[16], tv[16];
+                    load16_contig(cv, zh + L * N + 16 * g.t);
+                    load16_contig(tv, reinterpret_cast<const int32_t *>(row + C::PK_T1) + (size_t)i * N + 16 * g.t);
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m] - montmul(cv[m], tv[m]));
+                    intt16(acc, g.sm, g.gmask, g.t);
+                    int32_t w1[16];
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) {
+                        const int c = g.t + 16 * m;
+                        w1[m] = use_hint<MODE>(caddq(acc[m]), (hbits[c >> 5] >> (c & 31)) & 1u);
+                    }
+                    int32_t w1c[16];
+                    strided_to_contig(g, w1, w1c);
+                    uint32_t v[16];
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) v[m] = (uint32_t)w1c[m];
+                    pack16_words<PM::W1_BITS>(
+                        reinterpret_cast<uint32_t *>(slot + C::VS_W1 + (size_t)i * PM::POLYW1_PACKED + g.t * 2 * PM::W1_BITS), v);
+                    __syncwarp(g.gmask);
+                }
+            }
+        }
+        __syncthreads();
+
+        // c~' = H(mu || w1') and compare: thread per signature
+        if (tid < na) {
+            const unsigned it = base + tid;
+            const uint8_t *s = sig + (size_t)it * sig_pitch;
+            uint8_t *slot = my_slots + (size_t)tid * C::VSLOT;
+            uint32_t al[25], ah[25];
+            AlignedBytes src{slot + C::VS_MU, CRHBYTES + PM::W1PACKED_BYTES};
+            shake_absorb<SHAKE256_RATE>(al, ah, src, CRHBYTES + PM::W1PACKED_BYTES);
+            keccak_f1600(al, ah);
+            bool eq = true;
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const uint2 v = load_lane_bytes(s + 8 * w, 8);
+                eq &= (v.x == al[w]) && (v.y == ah[w]);
+            }
+            const int status = reinterpret_cast<const int *>(slot + C::VS_STATUS)[0];
+            ret[it] = (eq && status == 0) ? 0 : -1;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace cudil

@@ -1,0 +1,122 @@
+"""Fused engine: per-key resident caches + one persistent, graph-launched kernel per batch.
+
+Python host side of the ``cudil_engine_*`` C ABI (include/cudilithium.h).  A ``SignEngine`` /
+``VerifyEngine`` wraps one engine of one parameter set on the current CUDA device; messages are
+packed into one device buffer at 8-byte aligned offsets (``pack_messages``).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib
+
+
+def pack_messages(msgs: list[bytes] | np.ndarray, device="cuda"):
+    """Packs messages into one device buffer; returns (buffer, offsets, lengths) with every
+    offset a multiple of 8 (the engine reads message lanes as aligned 8-byte words)."""
+    if isinstance(msgs, np.ndarray):
+        msgs = [bytes(r) for r in msgs]
+    lens = np.array([len(m) for m in msgs], dtype=np.uint32)
+    offs = np.zeros(len(msgs), dtype=np.uint64)
+    pos = 0
+    for i, m in enumerate(msgs):
+        offs[i] = pos
+        pos += (len(m) + 7) // 8 * 8
+    host = np.zeros(max(pos, 8) + 8, dtype=np.uint8)
+    for i, m in enumerate(msgs):
+        host[int(offs[i]): int(offs[i]) + len(m)] = np.frombuffer(m, dtype=np.uint8)
+    return torch.from_numpy(host).to(device), offs, lens
+
+
+class Engine:
+    """One cudil_engine (one parameter set, current device)."""
+
+    def __init__(self, mode: int, max_keys: int, max_items: int, threads: int = 0, budget_bytes: int = 0):
+        self.mode = mode
+        self.params = _lib.params(mode)
+        self.max_keys, self.max_items = max_keys, max_items
+        h = ctypes.c_void_p()
+        check(lib.cudil_engine_create(ctypes.byref(h), mode, max_keys, max_items, threads, budget_bytes),
+              "cudil_engine_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.cudil_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        return lib.cudil_engine_device_bytes(self.h)
+
+    def info(self) -> dict:
+        m, t, sb, vb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lib.cudil_engine_info(self.h, ctypes.byref(m), ctypes.byref(t), ctypes.byref(sb), ctypes.byref(vb))
+        return {"mode": m.value, "threads": t.value, "sign_blocks": sb.value, "verify_blocks": vb.value}
+
+    def set_secret_keys(self, d_sk: torch.Tensor, stream=None):
+        n = d_sk.numel() // self.params.sk_bytes
+        check(lib.cudil_engine_set_secret_keys(self.h, d_sk.data_ptr(), n, _sp(stream)), "set_secret_keys")
+
+    def set_public_keys(self, d_pk: torch.Tensor, stream=None):
+        n = d_pk.numel() // self.params.pk_bytes
+        check(lib.cudil_engine_set_public_keys(self.h, d_pk.data_ptr(), n, _sp(stream)), "set_public_keys")
+
+    def sign(self, d_sig: torch.Tensor, d_msgs: torch.Tensor, offsets, mlens, key_idx, stream=None):
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        mlens = np.ascontiguousarray(mlens, dtype=np.uint32)
+        key_idx = np.ascontiguousarray(key_idx, dtype=np.uint32)
+        n = len(mlens)
+        check(lib.cudil_engine_sign(self.h, d_sig.data_ptr(), d_msgs.data_ptr(), d_msgs.numel(), offsets.ctypes.data,
+                                    mlens.ctypes.data, key_idx.ctypes.data, n, _sp(stream)), "cudil_engine_sign")
+
+    def verify(self, d_ret: torch.Tensor, d_sig: torch.Tensor, d_msgs: torch.Tensor, offsets, mlens, key_idx,
+               stream=None):
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        mlens = np.ascontiguousarray(mlens, dtype=np.uint32)
+        key_idx = np.ascontiguousarray(key_idx, dtype=np.uint32)
+        n = len(mlens)
+        check(lib.cudil_engine_verify(self.h, d_ret.data_ptr(), d_sig.data_ptr(), d_msgs.data_ptr(), d_msgs.numel(),
+                                      offsets.ctypes.data, mlens.ctypes.data, key_idx.ctypes.data, n, _sp(stream)),
+              "cudil_engine_verify")
+
+    def last_status(self) -> tuple[int, int]:
+        a, e = ctypes.c_ulonglong(), ctypes.c_uint32()
+        rc = lib.cudil_engine_last_status(self.h, ctypes.byref(a), ctypes.byref(e))
+        check(rc, "engine batch")
+        return a.value, e.value
+
+    # ---- numpy conveniences (synchronous)
+    def sign_np(self, msgs, key_idx) -> np.ndarray:
+        d_msgs, offs, lens = pack_messages(msgs)
+        n = len(lens)
+        d_sig = torch.empty(max(n, 1) * self.params.sig_bytes, dtype=torch.uint8, device="cuda")
+        self.sign(d_sig, d_msgs, offs, lens, key_idx)
+        torch.cuda.synchronize()
+        self.last_status()
+        return d_sig.cpu().numpy()[: n * self.params.sig_bytes].reshape(n, self.params.sig_bytes)
+
+    def verify_np(self, sig: np.ndarray, msgs, key_idx) -> np.ndarray:
+        d_msgs, offs, lens = pack_messages(msgs)
+        n = len(lens)
+        d_sig = torch.from_numpy(np.ascontiguousarray(sig, dtype=np.uint8).reshape(-1)).cuda()
+        d_ret = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+        self.verify(d_ret, d_sig, d_msgs, offs, lens, key_idx)
+        torch.cuda.synchronize()
+        return d_ret.cpu().numpy()[:n]
+
+
+def _sp(stream):
+    if stream is None:
+        return None
+    return stream if isinstance(stream, int) else stream.cuda_stream

@@ -129,6 +129,43 @@ int cudil_verify_noalloc(int mode, int *ret, const uint8_t *sig, size_t sig_pitc
  * invntt_tomont.  d_out may alias d_a. */
 int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t npolys, void *stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Fused engine (no reference counterpart; the reference re-expands A and re-transforms the
+ * secret key for every sign call and drives every rejection round from the host).
+ *
+ * One engine serves one parameter set on the current device.  It keeps, per key, the expanded
+ * matrix A_hat and the NTT-domain key material resident in device memory (secret keys: A_hat,
+ * s1_hat, s2_hat, t0_hat, rho, K, tr; public keys: A_hat, NTT(t1 * 2^d), tr) and runs a whole
+ * signing batch as one CUDA-graph launch around ONE persistent kernel whose device-side ticket
+ * queue hands every rejected attempt's slot the next (message, nonce) attempt.  Results are
+ * identical to cudil_sign / cudil_verify (deterministic signing: smallest accepted nonce).
+ *
+ * create:  allocates everything up front (max_keys cache rows of each kind, max_items messages per
+ *          batch, scratch for one persistent grid); CUDIL_ERR_BUDGET if that exceeds
+ *          device_budget_bytes (0 = no limit).  threads_per_block: 128 or 256 (0 = 256).
+ * sign/verify: d_msgs is one device buffer of msgs_bytes bytes holding every message at an 8-byte
+ *          aligned offset (offsets[i] + mlens[i] <= msgs_bytes, checked before any launch);
+ *          offsets / mlens / key_idx are HOST arrays of n entries (uploaded before the launch);
+ *          signatures are dense (sig_bytes each).  Asynchronous on `stream`; one batch in flight
+ *          per engine (calls on one engine must be ordered on one stream).
+ * last_status: attempts and error flags of the last completed batch (valid after sync);
+ *          returns CUDIL_ERR_TIMEOUT if a bounded device wait gave up. */
+typedef struct cudil_engine cudil_engine;
+int cudil_engine_create(cudil_engine **out, int mode, size_t max_keys, size_t max_items, int threads_per_block,
+                        size_t device_budget_bytes);
+int cudil_engine_destroy(cudil_engine *e);
+size_t cudil_engine_device_bytes(const cudil_engine *e);
+int cudil_engine_set_secret_keys(cudil_engine *e, const uint8_t *d_sk, size_t nkeys, void *stream);
+int cudil_engine_set_public_keys(cudil_engine *e, const uint8_t *d_pk, size_t nkeys, void *stream);
+int cudil_engine_sign(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
+                      const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
+                      void *stream);
+int cudil_engine_verify(cudil_engine *e, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
+                        const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
+                        void *stream);
+int cudil_engine_last_status(const cudil_engine *e, unsigned long long *attempts, unsigned *error);
+int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks);
+
 /* Peak of the 32-bit LOP3/funnel-shift mix Keccak-f[1600] issues: launches `blocks` x 256 threads
  * doing `iters` x 32 ALU operations each; *ops_per_launch receives the operation count. */
 int cudil_alu_peak(uint32_t *d_out, int blocks, int iters, void *stream, double *ops_per_launch);

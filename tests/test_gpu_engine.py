@@ -1,0 +1,126 @@
+"""Fused engine (persistent kernel + per-key caches + graph) vs the CPU oracle (needs a B200)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MODES = [2, 3, 5]
+
+
+def rand_msgs(rng, n, lens):
+    return [bytes(rng.integers(0, 256, int(l), dtype=np.uint8)) for l in lens]
+
+
+def oracle_sign(oracle, mode, sk, key_idx, msgs):
+    out = []
+    for i, m in enumerate(msgs):
+        arr = np.frombuffer(m, dtype=np.uint8).reshape(1, -1) if m else np.zeros((1, 0), np.uint8)
+        out.append(oracle.sign_batch(mode, arr, sk[key_idx[i]: key_idx[i] + 1])[0])
+    return np.stack(out)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("threads", [128, 256])
+def test_engine_sign_matches_oracle(cuda_ok, oracle, mode, threads):
+    import torch
+    from cudilithium_b200.engine import Engine
+    rng = np.random.default_rng(mode * 10 + threads)
+    nk, n = 7, 150
+    pk, sk = oracle.keypair_batch(mode, nk, rand_index=500 + mode)
+    lens = rng.integers(0, 300, n)
+    lens[:6] = [0, 1, 135, 136, 137, 8]
+    msgs = rand_msgs(rng, n, lens)
+    key_idx = rng.integers(0, nk, n).astype(np.uint32)
+    eng = Engine(mode, max_keys=nk, max_items=n, threads=threads)
+    eng.set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
+    sig = eng.sign_np(msgs, key_idx)
+    want = oracle_sign(oracle, mode, sk, key_idx, msgs)
+    assert np.array_equal(sig, want)
+    # second, smaller batch through the same graph (batch size lives in device memory)
+    sig2 = eng.sign_np(msgs[:17], key_idx[:17])
+    assert np.array_equal(sig2, want[:17])
+    attempts, err = eng.last_status()
+    assert err == 0 and attempts >= 17
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_engine_verify_matches_oracle(cuda_ok, oracle, mode):
+    import torch
+    from cudilithium_b200.engine import Engine
+    rng = np.random.default_rng(70 + mode)
+    nk, n = 5, 200
+    p = oracle.params(mode)
+    pk, sk = oracle.keypair_batch(mode, nk, rand_index=900 + mode)
+    lens = rng.integers(0, 200, n)
+    msgs = rand_msgs(rng, n, lens)
+    key_idx = rng.integers(0, nk, n).astype(np.uint32)
+    sig = oracle_sign(oracle, mode, sk, key_idx, msgs)
+    flip = rng.permutation(n)[: n // 10]
+    for i in flip:
+        sig[i, int(rng.integers(0, p.sig_bytes))] ^= np.uint8(1 << int(rng.integers(0, 8)))
+    eng = Engine(mode, max_keys=nk, max_items=n)
+    eng.set_public_keys(torch.from_numpy(pk.reshape(-1)).cuda())
+    ret = eng.verify_np(sig, msgs, key_idx)
+    want = np.array([oracle.verify_batch(mode, sig[i:i + 1],
+                                         np.frombuffer(msgs[i], np.uint8).reshape(1, -1) if msgs[i] else np.zeros((1, 0), np.uint8),
+                                         pk[key_idx[i]: key_idx[i] + 1])[0] for i in range(n)])
+    assert np.array_equal(ret, want)
+    assert np.all(ret[flip] == -1)
+
+
+def test_engine_matches_plain_path_large_batch(cuda_ok, oracle):
+    """Dilithium2, 4000 messages over 300 keys: fused engine == plain stage-by-stage path."""
+    import torch
+    from cudilithium_b200 import Dilithium
+    from cudilithium_b200.engine import Engine
+    mode, nk, n = 2, 300, 4000
+    d = Dilithium(mode)
+    pk, sk = d.keypair(nk, rand_index=77)
+    rng = np.random.default_rng(5)
+    key_idx = rng.integers(0, nk, n).astype(np.uint32)
+    m = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    plain = d.sign(m, sk[key_idx], exec_threshold=4096)
+    eng = Engine(mode, max_keys=nk, max_items=n)
+    eng.set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
+    fused = eng.sign_np(m, key_idx)
+    assert np.array_equal(fused, plain)
+    veng = Engine(mode, max_keys=nk, max_items=n)
+    veng.set_public_keys(torch.from_numpy(pk.reshape(-1)).cuda())
+    assert np.all(veng.verify_np(fused, m, key_idx) == 0)
+
+
+def test_engine_long_messages(cuda_ok, oracle):
+    """Dilithium3 with message lengths up to 64 KiB (log-uniform), as the long-message workload."""
+    import torch
+    from cudilithium_b200.engine import Engine
+    mode, nk, n = 3, 4, 24
+    pk, sk = oracle.keypair_batch(mode, nk, rand_index=31)
+    rng = np.random.default_rng(9)
+    lens = np.floor(np.exp(rng.uniform(np.log(32), np.log(65536), n))).astype(int)
+    lens[0] = 65536
+    msgs = rand_msgs(rng, n, lens)
+    key_idx = (np.arange(n) % nk).astype(np.uint32)
+    eng = Engine(mode, max_keys=nk, max_items=n)
+    eng.set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
+    assert np.array_equal(eng.sign_np(msgs, key_idx), oracle_sign(oracle, mode, sk, key_idx, msgs))
+
+
+def test_engine_argument_errors(cuda_ok, oracle):
+    import torch
+    from cudilithium_b200 import CudilError
+    from cudilithium_b200._lib import CUDIL_ERR_BUDGET
+    from cudilithium_b200.engine import Engine, pack_messages
+    pk, sk = oracle.keypair_batch(2, 2)
+    eng = Engine(2, max_keys=2, max_items=8)
+    eng.set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
+    d_msgs, offs, lens = pack_messages([b"abc"] * 4)
+    d_sig = torch.empty(4 * 2420, dtype=torch.uint8, device="cuda")
+    with pytest.raises(CudilError):
+        eng.sign(d_sig, d_msgs, offs, lens, [0, 1, 2, 0])      # key index out of range
+    with pytest.raises(CudilError):
+        eng.sign(d_sig, d_msgs, offs + 1, lens, [0, 0, 0, 0])  # misaligned message offsets
+    with pytest.raises(CudilError):
+        eng.sign(d_sig, d_msgs, np.zeros(9, np.uint64), np.zeros(9, np.uint32), np.zeros(9, np.uint32))  # > max_items
+    with pytest.raises(CudilError) as ei:
+        Engine(5, max_keys=4096, max_items=65536, budget_bytes=1 << 20)
+    assert ei.value.code == CUDIL_ERR_BUDGET
