@@ -1,17 +1,22 @@
 #!/usr/bin/env python3
 """Benchmark of the batched Dilithium path on B200 (one JSON line on rank 0).
 
-Default workload: Dilithium2 batched signing of a batch of 10000 32-byte messages, one key per
-message (the reference's bench_dilithium batch, benches/bench_dilithium.cu:277-296), keys from
-the reference's seed scheme SHAKE128(le64(2i+1)).  A step = one sign call over the whole batch
-followed by one verify call over the produced signatures.
+Headline workload: Dilithium2 batched signing of 10000 32-byte messages, one key per message (the
+reference's bench_dilithium batch, benches/bench_dilithium.cu:277-296), keys from the reference's
+seed scheme SHAKE128(le64(2i+1)).  A step = the fused engine building the batch's key caches and
+signing the batch in one graph launch (then verifying it against freshly built public-key caches).
 
-  value         Dilithium2 signatures/s with inputs resident in HBM (device-pointer C-ABI calls)
-  e2e           the same through the public host-buffer C ABI (cudil_sign / cudil_verify with
-                pinned host buffers; H2D of m, sk and D2H of sig inside the timed region)
-  verify_per_s  verifications/s of the same step (device-resident)
-  roofline      dominant kernel of the step: algorithmic 32-bit ALU operations per launch over its
-                CUDA-event duration, against the measured LOP3/SHF issue peak of this GPU
+  value         Dilithium2 signatures/s of the fused engine, inputs resident in HBM
+  plain         the same batch through the plain stage-by-stage path (cudil_sign_dev /
+                cudil_verify_dev, best exec threshold of --thresholds); fused_over_plain = ratio
+  e2e           fused signing with pinned host inputs/outputs: H2D of m and sk, D2H of the
+                signatures inside the timed region
+  verify_per_s  verifications/s of the same step (fused engine, public-key caches built per step)
+  roofline      the persistent signing kernel: algorithmic 32-bit ALU operations (work model below,
+                attempts counted on the device) over its CUDA-event duration, against the measured
+                LOP3/SHF issue peak of this GPU
+  configs       configs 1-4 of the workload list (batch-1024 latency, NTT microbench vs HBM peak,
+                Dilithium3 log-uniform messages, Dilithium5 cached-key verification with 10% bit flips)
   cpu_baseline  the CPU oracle (C restatement, OpenMP over all host cores) on a bounded sample
 
 --impl reference runs the CPU implementation of the same path (the oracle; the reference ships no
@@ -151,32 +156,42 @@ def run_reference(args) -> dict:
 
 
 # ---------------------------------------------------------------------------- GPU leg
-def kernel_ops(name: str, launches: int, mode: int, batch: int, nexec_total: int, mlen: int, pm) -> float | None:
-    """Algorithmic ALU operations of all launches of one kernel in the instrumented step."""
+def sign_attempt_ops(pm, attempts: int, reject_intt: int) -> float:
+    """Algorithmic 32-bit ALU operations of the signing attempts of one batch (work the
+    deterministic signing algorithm performs on these attempts, early exits included)."""
     K, L, w1 = pm.k, pm.l, pm.k * pm.polyw1_packed
-    blocks = lambda nbytes: nbytes // 136 + 1  # SHAKE256 absorb permutations incl. padding
-    if name == "k_expand_a":
-        return 2 * batch * K * L * 5 * OPS_PERM  # sign setup + verify
-    if name == "k_sign_expand_mask":
-        return nexec_total * L * 5 * OPS_PERM
-    if name == "k_sign_challenge":
-        return nexec_total * (blocks(64 + w1) + 1) * OPS_PERM
-    if name == "k_sign_compute_w":
-        return nexec_total * (L * OPS_NTT_FWD + K * OPS_NTT_INV + K * L * 256 * OPS_PW)
-    if name == "k_sign_prehash":
-        return batch * (blocks(32 + mlen) + 1) * OPS_PERM
-    if name == "k_verify_prepare":
-        return batch * (blocks(pm.pk_bytes) + blocks(32 + mlen) + 1) * OPS_PERM
-    if name == "k_verify_final":
-        return batch * blocks(64 + w1) * OPS_PERM
-    if name == "k_verify_w":
-        return batch * ((L + 1 + K) * OPS_NTT_FWD + K * OPS_NTT_INV + (K * L + K) * 256 * OPS_PW)
-    if name == "k_sign_unpack_ntt":
-        return batch * (L + 2 * K) * OPS_NTT_FWD
-    return None
+    perms = L * 5 + (64 + w1) // 136 + 1 + 1          # ExpandMask, c~ absorb, SampleInBall
+    per_attempt = (perms * OPS_PERM + L * OPS_NTT_FWD + K * OPS_NTT_INV + K * L * 256 * OPS_PW  # w = A y
+                   + OPS_NTT_FWD)                                                              # NTT(c)
+    return attempts * per_attempt + reject_intt * (OPS_NTT_INV + 256 * OPS_PW)
+
+
+def cache_ops(pm, nkeys: int) -> float:
+    """ExpandA (K*L entries of 5 SHAKE128 blocks) + NTT of s1, s2, t0 per key."""
+    return nkeys * (pm.k * pm.l * 5 * OPS_PERM + (pm.l + 2 * pm.k) * OPS_NTT_FWD)
+
+
+class Timer:
+    def __init__(self, torch, stream):
+        self.torch, self.st, self.pairs = torch, stream, []
+
+    def __enter__(self):
+        self.a = self.torch.cuda.Event(enable_timing=True)
+        self.b = self.torch.cuda.Event(enable_timing=True)
+        self.a.record(self.st)
+        return self
+
+    def __exit__(self, *exc):
+        self.b.record(self.st)
+        self.pairs.append((self.a, self.b))
+
+    def total_ms(self):
+        return sum(a.elapsed_time(b) for a, b in self.pairs)
 
 
 def run_gpu(args) -> dict | None:
+    import ctypes
+
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -191,165 +206,216 @@ def run_gpu(args) -> dict | None:
     import cudilithium_b200 as cd
     from cudilithium_b200 import _lib
     from cudilithium_b200.api import TaskLut, alloc_pool, pinned
+    from cudilithium_b200.engine import Engine, pack_messages
 
     lib = _lib.lib
-    mode, B, T = args.mode, args.batch, args.threshold
+    mode, B = args.mode, args.batch
     d = cd.Dilithium(mode)
     pm = d.params
     dev = torch.device("cuda", local)
     st = torch.cuda.current_stream()
-    sp_ptr = st.cuda_stream
-
-    # ---- inputs (reference seed scheme; each rank signs its own batch of the same shape)
-    t0 = time.perf_counter()
-    kp_pool, kpp = alloc_pool(d.keypair_row_bytes(), B)
-    d_pk = torch.empty(B * pm.pk_bytes, dtype=torch.uint8, device=dev)
-    d_sk = torch.empty(B * pm.sk_bytes, dtype=torch.uint8, device=dev)
-    _lib.check(lib.cudil_keypair_dev(mode, d_pk.data_ptr(), d_sk.data_ptr(), None, kp_pool.data_ptr(), kpp, B,
-                                     sp_ptr, rank * 2 * B), "keypair")
-    torch.cuda.synchronize()
-    kg_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    kg_ev[0].record(st)
-    _lib.check(lib.cudil_keypair_dev(mode, d_pk.data_ptr(), d_sk.data_ptr(), None, kp_pool.data_ptr(), kpp, B,
-                                     sp_ptr, rank * 2 * B), "keypair")
-    kg_ev[1].record(st)
-    torch.cuda.synchronize()
-    keygen_ms = kg_ev[0].elapsed_time(kg_ev[1])
-    del kp_pool
-    rng = np.random.default_rng(1234 + rank)
-    m_host = rng.integers(0, 256, (B, MLEN), dtype=np.uint8)
-    d_m = torch.from_numpy(m_host.reshape(-1)).to(dev)
-    d_sig = torch.empty(B * pm.sig_bytes, dtype=torch.uint8, device=dev)
-    d_ret = torch.empty(B, dtype=torch.int32, device=dev)
-    s_pool, sp = alloc_pool(d.sign_row_bytes(MLEN), B)
-    t_pool, tp = alloc_pool(d.sign_temp_row_bytes(), T)
-    v_pool, vp = alloc_pool(d.verify_row_bytes(MLEN), B)
-    lut = TaskLut(B, T)
-    log(f"[bench] rank {rank}: inputs ready in {time.perf_counter() - t0:.1f}s "
-        f"(pools {(s_pool.numel() + t_pool.numel() + v_pool.numel()) / 2**20:.0f} MiB)")
-
-    def sign_dev():
-        _lib.check(lib.cudil_sign_dev(mode, d_sig.data_ptr(), pm.sig_bytes, d_m.data_ptr(), MLEN, MLEN,
-                                      d_sk.data_ptr(), s_pool.data_ptr(), sp, t_pool.data_ptr(), tp,
-                                      ctypes_byref(lut.c), T, B, sp_ptr), "sign")
-
-    def verify_dev():
-        _lib.check(lib.cudil_verify_dev(mode, d_ret.data_ptr(), d_sig.data_ptr(), pm.sig_bytes, pm.sig_bytes,
-                                        d_m.data_ptr(), MLEN, MLEN, d_pk.data_ptr(), v_pool.data_ptr(), vp, B,
-                                        sp_ptr), "verify")
+    spp = st.cuda_stream
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        sign_dev()
-        verify_dev()
-    barrier()
-    # correctness of the timed configuration: every produced signature verifies
-    assert int((d_ret != 0).sum().item()) == 0, "warm-up signatures failed to verify"
+    def max_over_ranks(*vals):
+        if world == 1:
+            return vals
+        t = torch.tensor(vals, dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return tuple(t.tolist())
 
-    # ---- timed region: K steps, device-resident inputs
+    # ---- inputs: keys from the reference seed scheme, one key per message
+    kp_pool, kpp = alloc_pool(d.keypair_row_bytes(), B)
+    d_pk = torch.empty(B * pm.pk_bytes, dtype=torch.uint8, device=dev)
+    d_sk = torch.empty(B * pm.sk_bytes, dtype=torch.uint8, device=dev)
+    kg = Timer(torch, st)
+    for _ in range(2):
+        with kg:
+            _lib.check(lib.cudil_keypair_dev(mode, d_pk.data_ptr(), d_sk.data_ptr(), None, kp_pool.data_ptr(), kpp,
+                                             B, spp, rank * 2 * B), "keypair")
+    torch.cuda.synchronize()
+    keygen_ms = kg.pairs[-1][0].elapsed_time(kg.pairs[-1][1])
+    del kp_pool
+    rng = np.random.default_rng(1234 + rank)
+    m_host = rng.integers(0, 256, (B, MLEN), dtype=np.uint8)
+    d_m = torch.from_numpy(m_host.reshape(-1)).to(dev)
+    keys = np.arange(B, dtype=np.uint32)
+    offs = (np.arange(B, dtype=np.uint64) * MLEN)
+    lens = np.full(B, MLEN, dtype=np.uint32)
+
+    # ---- plain stage-by-stage path (cudil_sign_dev / cudil_verify_dev), best exec threshold
+    p_sig = torch.empty(B * pm.sig_bytes, dtype=torch.uint8, device=dev)
+    p_ret = torch.empty(B, dtype=torch.int32, device=dev)
+    s_pool, sp = alloc_pool(d.sign_row_bytes(MLEN), B)
+    v_pool, vp = alloc_pool(d.verify_row_bytes(MLEN), B)
+    tmax = max(args.thresholds)
+    t_pool, tp = alloc_pool(d.sign_temp_row_bytes(), tmax)
+
+    def plain_sign(T, lut):
+        _lib.check(lib.cudil_sign_dev(mode, p_sig.data_ptr(), pm.sig_bytes, d_m.data_ptr(), MLEN, MLEN,
+                                      d_sk.data_ptr(), s_pool.data_ptr(), sp, t_pool.data_ptr(), tp,
+                                      ctypes.byref(lut.c), T, B, spp), "sign")
+
+    def plain_verify():
+        _lib.check(lib.cudil_verify_dev(mode, p_ret.data_ptr(), p_sig.data_ptr(), pm.sig_bytes, pm.sig_bytes,
+                                        d_m.data_ptr(), MLEN, MLEN, d_pk.data_ptr(), v_pool.data_ptr(), vp, B,
+                                        spp), "verify")
+
+    luts = {T: TaskLut(B, T) for T in args.thresholds}
+    best_T, best_ms = None, None
+    for T in args.thresholds:
+        plain_sign(T, luts[T])
+        tm = Timer(torch, st)
+        with tm:
+            plain_sign(T, luts[T])
+        torch.cuda.synchronize()
+        ms = tm.total_ms()
+        if best_ms is None or ms < best_ms:
+            best_T, best_ms = T, ms
+    for _ in range(args.warmup):
+        plain_sign(best_T, luts[best_T])
+        plain_verify()
+    barrier()
+    tps, tpv = Timer(torch, st), Timer(torch, st)
+    for _ in range(args.steps):
+        with tps:
+            plain_sign(best_T, luts[best_T])
+        with tpv:
+            plain_verify()
+    barrier()
+    plain_sign_ms, plain_verify_ms = max_over_ranks(tps.total_ms(), tpv.total_ms())
+    plain_ok = int((p_ret != 0).sum().item()) == 0
+    plain_sign_rate = world * B * args.steps / (plain_sign_ms / 1e3)
+    plain_verify_rate = world * B * args.steps / (plain_verify_ms / 1e3)
+
+    # ---- fused engine: per step the key caches are built for this batch's keys (each key signs
+    # once here, so the cache build is part of the per-signature work) and one graph launch signs
+    es = Engine(mode, max_keys=B, max_items=B, threads=args.engine_threads)
+    ev = Engine(mode, max_keys=B, max_items=B, threads=args.engine_threads)
+    f_sig = torch.empty(B * pm.sig_bytes, dtype=torch.uint8, device=dev)
+    f_ret = torch.empty(B, dtype=torch.int32, device=dev)
+
+    def fused_sign():
+        es.set_secret_keys(d_sk, stream=spp)
+        es.sign(f_sig, d_m, offs, lens, keys, stream=spp)
+
+    def fused_verify():
+        ev.set_public_keys(d_pk, stream=spp)
+        ev.verify(f_ret, f_sig, d_m, offs, lens, keys, stream=spp)
+
+    for _ in range(args.warmup):
+        fused_sign()
+        fused_verify()
+    barrier()
+    assert torch.equal(f_sig, p_sig), "fused and plain signatures differ"
+    assert int((f_ret != 0).sum().item()) == 0, "fused verify rejected valid signatures"
+
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
     launches0 = lib.cudil_launch_count()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    tfs, tfv = Timer(torch, st), Timer(torch, st)
     barrier()
     wall0 = time.perf_counter()
-    for a, b, c in ev:
-        a.record(st)
-        sign_dev()
-        b.record(st)
-        verify_dev()
-        c.record(st)
+    for _ in range(args.steps):
+        with tfs:
+            fused_sign()
+        with tfv:
+            fused_verify()
     barrier()
     wall = time.perf_counter() - wall0
     launches = lib.cudil_launch_count() - launches0
     clk = clocks.stop()
-    sign_ms = sum(a.elapsed_time(b) for a, b, _ in ev)
-    verify_ms = sum(b.elapsed_time(c) for _, b, c in ev)
-    step_ms = sum(a.elapsed_time(c) for a, _, c in ev)
-    if world > 1:
-        t = torch.tensor([sign_ms, verify_ms, step_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sign_ms, verify_ms, step_ms = t.tolist()
-    value = world * B * args.steps / (sign_ms / 1e3)
-    verify_rate = world * B * args.steps / (verify_ms / 1e3)
-    ok = int((d_ret != 0).sum().item()) == 0
+    fs_ms, fv_ms = max_over_ranks(tfs.total_ms(), tfv.total_ms())
+    value = world * B * args.steps / (fs_ms / 1e3)
+    verify_rate = world * B * args.steps / (fv_ms / 1e3)
+    attempts, reject_intt = es.last_work()
+    fused_ok = torch.equal(f_sig, p_sig) and int((f_ret != 0).sum().item()) == 0
 
-    # ---- e2e through the host-buffer C ABI
+    # ---- e2e: host buffers in, host signatures out, through the same engine
     h_m = pinned(B * MLEN)
     h_m.numpy()[:] = m_host.reshape(-1)
     h_sk = pinned(B * pm.sk_bytes)
     h_sk.copy_(d_sk.cpu())
-    h_pk = pinned(B * pm.pk_bytes)
-    h_pk.copy_(d_pk.cpu())
     h_sig = pinned(B * pm.sig_bytes)
-    h_ret = torch.empty(B, dtype=torch.int32, pin_memory=True)
-    siglen = __import__("ctypes").c_size_t(0)
+    e_m = torch.empty_like(d_m)
+    e_sk = torch.empty_like(d_sk)
+    e_sig = torch.empty_like(f_sig)
 
-    def sign_host():
-        _lib.check(lib.cudil_sign(mode, h_sig.data_ptr(), pm.sig_bytes, ctypes_byref(siglen), h_m.data_ptr(), MLEN,
-                                  MLEN, h_sk.data_ptr(), s_pool.data_ptr(), sp, t_pool.data_ptr(), tp,
-                                  ctypes_byref(lut.c), T, B, sp_ptr), "sign(host)")
+    def e2e_step():
+        e_m.copy_(h_m, non_blocking=True)
+        e_sk.copy_(h_sk, non_blocking=True)
+        es.set_secret_keys(e_sk, stream=spp)
+        es.sign(e_sig, e_m, offs, lens, keys, stream=spp)
+        h_sig.copy_(e_sig, non_blocking=True)
 
-    sign_host()
+    e2e_step()
     barrier()
-    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for a, b in e2e_ev:
-        a.record(st)
-        sign_host()
-        b.record(st)
+    te = Timer(torch, st)
+    for _ in range(args.steps):
+        with te:
+            e2e_step()
     barrier()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = t.item()
+    (e2e_ms,) = max_over_ranks(te.total_ms())
+    assert torch.equal(h_sig, p_sig.cpu()), "e2e signatures differ"
     e2e = world * B * args.steps / (e2e_ms / 1e3)
 
-    # ---- roofline: one instrumented step, per-kernel CUDA events on the launch stream
-    peak_ops = measure_alu_peak(lib, dev, sp_ptr)
+    # ---- roofline: one instrumented fused signing step
+    peak_ops = measure_alu_peak(lib, dev, spp)
     lib.cudil_kernel_stats_reset()
     lib.cudil_kernel_timing(1)
-    sign_dev()
-    verify_dev()
+    fused_sign()
     torch.cuda.synchronize()
     lib.cudil_kernel_timing(0)
     stats = _lib.kernel_stats()
-    nexec_total = stats.get("k_sign_expand_mask", (0, 0))[1] * T
+    att1, intt1 = es.last_work()
+    g_ms = stats.get("k_fused_sign (graph)", (0.0, 1))[0]
+    sign_ops = sign_attempt_ops(pm, att1, intt1) + B * 2 * OPS_PERM  # + mu, rho' prologue
+    c_ms = stats.get("k_cache_sk", (0.0, 1))[0] + stats.get("k_expand_a", (0.0, 1))[0]
+    achieved = sign_ops / (g_ms / 1e3) / 1e9 if g_ms else None
     total_ms = sum(v[0] for v in stats.values())
-    dom = max(stats.items(), key=lambda kv: kv[1][0])
-    name, (ms, n_launch) = dom
-    ops = kernel_ops(name, n_launch, mode, B, nexec_total, MLEN, pm)
-    achieved = (ops / n_launch) / (ms / n_launch / 1e3) / 1e9 if ops else None
     roofline = {
-        "bound": "int32-alu", "kernel": name, "achieved": achieved, "peak": peak_ops / 1e9, "unit": "Gop/s",
-        "frac": (achieved / (peak_ops / 1e9)) if achieved else None, "traffic": None,
-        "ms_per_launch": ms / n_launch, "launches": n_launch,
-        "share_of_step": ms / total_ms if total_ms else None,
-        "peak_source": "measured live: k_alu_peak (3 LOP3 : 1 SHF, the Keccak mix)",
+        "bound": "int32-alu", "kernel": "k_fused_sign (persistent, graph with init + prehash)",
+        "achieved": achieved, "peak": peak_ops / 1e9, "unit": "Gop/s",
+        "frac": achieved / (peak_ops / 1e9) if achieved else None, "traffic": None,
+        "ms_per_launch": g_ms, "launches": 1, "share_of_step": g_ms / total_ms if total_ms else None,
+        "attempts": att1, "reject_intt": intt1,
+        "ops_model": "Keccak-f1600 = 4560 LOP3/SHF ops; NTT 6144, invNTT 7168, Montgomery product 5",
+        "peak_source": "measured live: k_alu_peak (3 LOP3 : 1 SHF at 64 ops/clk/SM; IMAD-heavy NTT work can "
+                       "co-issue on the FMA pipe, so frac may exceed 1)",
+        "cache_build": {"ms": c_ms, "achieved_gops": cache_ops(pm, B) / (c_ms / 1e3) / 1e9 if c_ms else None},
         "kernels": {k: {"ms": round(v[0], 4), "launches": v[1]} for k, v in sorted(stats.items(), key=lambda kv: -kv[1][0])},
     }
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": (fs_ms + fv_ms) / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic: keys from the reference seed scheme, uniform random 32-byte messages",
-        "config": {"workload": f"Dilithium{mode} batched sign + verify, batch {B} (reference bench batch), "
-                               f"{MLEN}-byte messages, one key per message", "batch": B, "mlen": MLEN,
-                   "path": "plain stage-by-stage (cudil_sign_dev / cudil_verify_dev)", "exec_threshold": T,
-                   "l2": "inputs larger than L2: sign pool rows alone are "
-                         f"{s_pool.numel() / 2**20:.0f} MiB per rank", "parallelism": f"replicas x{world}"},
-        "verify_per_s": verify_rate, "keygen_per_s": B / (keygen_ms / 1e3), "all_verified": ok,
-        "attempts_per_signature": nexec_total / B if B else None,
+        "config": {"workload": f"Dilithium{mode} batched sign (+ verify), batch {B} (the reference bench batch), "
+                               f"{MLEN}-byte messages, one key per message; per step the fused engine builds the "
+                               f"batch's key caches and signs in one graph launch", "batch": B, "mlen": MLEN,
+                   "path": "fused engine (persistent k_fused_sign, CUDA graph)",
+                   "engine": es.info(),
+                   "l2": f"inputs larger than L2: the batch's secret-key caches alone are "
+                         f"{B * (pm.k * pm.l + pm.l + 2 * pm.k) * 1024 / 2**20:.0f} MiB per rank",
+                   "parallelism": f"replicas x{world}"},
+        "verify_per_s": verify_rate, "keygen_per_s": world * B / (keygen_ms / 1e3),
+        "plain": {"sign_per_s": plain_sign_rate, "verify_per_s": plain_verify_rate, "exec_threshold": best_T,
+                  "all_verified": plain_ok},
+        "fused_over_plain": {"sign": value / plain_sign_rate, "verify": verify_rate / plain_verify_rate},
+        "bit_exact_fused_vs_plain": fused_ok, "attempts_per_signature": attempts / B,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * (MLEN + pm.sk_bytes),
                 "d2h_bytes_per_step": B * pm.sig_bytes},
         "gpu_launches": int(launches), "wall_s_timed": wall, "clocks": clk, "roofline": roofline,
     }
+    del s_pool, v_pool, t_pool, es, ev
+    torch.cuda.empty_cache()
+    if not args.quick:
+        result["configs"] = run_configs(args, torch, np, lib, _lib, dev, spp, rank)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -357,6 +423,195 @@ def run_gpu(args) -> dict | None:
         rate, sample, cores = cpu_sign_rate(mode, args.cpu_seconds)
         result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     return result if rank == 0 else None
+
+
+def run_configs(args, torch, np, lib, _lib, dev, spp, rank) -> dict:
+    """The other configurations, reported beside the headline (not the bench value)."""
+    import ctypes
+
+    import cudilithium_b200 as cd
+    from cudilithium_b200.api import TaskLut, alloc_pool, ntt_mul
+    from cudilithium_b200.engine import Engine, pack_messages
+    st = torch.cuda.current_stream()
+    out = {}
+
+    # config 1: Dilithium2 keygen + sign + verify, batch 1024 (latency of each batch call)
+    d = cd.Dilithium(2)
+    pm = d.params
+    n = 1024
+    pool, kpp = alloc_pool(d.keypair_row_bytes(), n)
+    pk = torch.empty(n * pm.pk_bytes, dtype=torch.uint8, device=dev)
+    sk = torch.empty(n * pm.sk_bytes, dtype=torch.uint8, device=dev)
+    m = torch.randint(0, 256, (n * 32,), dtype=torch.uint8, device=dev)
+    offs, lens, keys = np.arange(n, dtype=np.uint64) * 32, np.full(n, 32, np.uint32), np.arange(n, dtype=np.uint32)
+    s_pool, sp = alloc_pool(d.sign_row_bytes(32), n)
+    t_pool, tp = alloc_pool(d.sign_temp_row_bytes(), 4096)
+    v_pool, vp = alloc_pool(d.verify_row_bytes(32), n)
+    lut = TaskLut(n, 4096)
+    sig = torch.empty(n * pm.sig_bytes, dtype=torch.uint8, device=dev)
+    ret = torch.empty(n, dtype=torch.int32, device=dev)
+    es, ev = Engine(2, n, n), Engine(2, n, n)
+
+    def c1_plain():
+        lib.cudil_keypair_dev(2, pk.data_ptr(), sk.data_ptr(), None, pool.data_ptr(), kpp, n, spp, 0)
+        lib.cudil_sign_dev(2, sig.data_ptr(), pm.sig_bytes, m.data_ptr(), 32, 32, sk.data_ptr(), s_pool.data_ptr(),
+                           sp, t_pool.data_ptr(), tp, ctypes.byref(lut.c), 4096, n, spp)
+        lib.cudil_verify_dev(2, ret.data_ptr(), sig.data_ptr(), pm.sig_bytes, pm.sig_bytes, m.data_ptr(), 32, 32,
+                             pk.data_ptr(), v_pool.data_ptr(), vp, n, spp)
+
+    def c1_fused():
+        lib.cudil_keypair_dev(2, pk.data_ptr(), sk.data_ptr(), None, pool.data_ptr(), kpp, n, spp, 0)
+        es.set_secret_keys(sk, stream=spp)
+        es.sign(sig, m, offs, lens, keys, stream=spp)
+        ev.set_public_keys(pk, stream=spp)
+        ev.verify(ret, sig, m, offs, lens, keys, stream=spp)
+
+    res = {}
+    for name, fn in (("plain", c1_plain), ("fused", c1_fused)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        tm = Timer(torch, st)
+        for _ in range(5):
+            with tm:
+                fn()
+        torch.cuda.synchronize()
+        res[name + "_ms"] = tm.total_ms() / 5
+        assert int((ret != 0).sum().item()) == 0
+    res["speedup"] = res["plain_ms"] / res["fused_ms"]
+    out["d2_keygen_sign_verify_batch1024"] = res
+    del pool, s_pool, t_pool, v_pool, es, ev
+
+    # config 2: NTT microbench, 2^20 polynomials: NTT -> Montgomery product -> invNTT
+    npoly = 1 << 20
+    g = torch.Generator(device=dev).manual_seed(42)
+    a = torch.randint(0, 8380417, (npoly, 256), dtype=torch.int32, device=dev, generator=g)
+    b = torch.randint(0, 8380417, (npoly, 256), dtype=torch.int32, device=dev, generator=g)
+    o = torch.empty_like(a)
+    for _ in range(3):
+        ntt_mul(a, b, o)
+    torch.cuda.synchronize()
+    tm = Timer(torch, st)
+    for _ in range(10):
+        with tm:
+            ntt_mul(a, b, o)
+    torch.cuda.synchronize()
+    ms = tm.total_ms() / 10
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    gbs = npoly * 3072 / (ms / 1e3) / 1e9
+    out["ntt_microbench_2^20"] = {"ms": ms, "polys_per_s": npoly / (ms / 1e3), "hbm_gbs": gbs,
+                                  "hbm_frac": gbs / hbm, "hbm_peak_gbs": hbm,
+                                  "peak_source": "MEASURED_PEAKS.json" if peaks else "fallback 6650",
+                                  "bytes_per_poly": 3072, "l2": "inputs 2 GiB > L2"}
+    del a, b, o
+
+    # config 3: Dilithium3 signing of 16384 messages over 1024 keys, log-uniform 32 B .. 64 KiB
+    d3 = cd.Dilithium(3)
+    p3 = d3.params
+    nk, nm = 1024, 16384
+    pool, kpp = alloc_pool(d3.keypair_row_bytes(), nk)
+    pk3 = torch.empty(nk * p3.pk_bytes, dtype=torch.uint8, device=dev)
+    sk3 = torch.empty(nk * p3.sk_bytes, dtype=torch.uint8, device=dev)
+    lib.cudil_keypair_dev(3, pk3.data_ptr(), sk3.data_ptr(), None, pool.data_ptr(), kpp, nk, spp, 0)
+    del pool
+    rng = np.random.default_rng(3)
+    mlens = np.floor(np.exp(rng.uniform(np.log(32), np.log(65536), nm))).astype(np.uint32)
+    offs3 = np.zeros(nm, np.uint64)
+    offs3[1:] = np.cumsum((mlens[:-1].astype(np.uint64) + 7) // 8 * 8)
+    total = int(offs3[-1] + mlens[-1]) + 8
+    d_msgs = torch.randint(0, 256, (total,), dtype=torch.uint8, device=dev)
+    keys3 = (np.arange(nm) % nk).astype(np.uint32)
+    e3 = Engine(3, nk, nm)
+    s3 = torch.empty(nm * p3.sig_bytes, dtype=torch.uint8, device=dev)
+    e3.set_secret_keys(sk3, stream=spp)
+    for _ in range(3):
+        e3.sign(s3, d_msgs, offs3, mlens, keys3, stream=spp)
+    torch.cuda.synchronize()
+    tm, tc = Timer(torch, st), Timer(torch, st)
+    for _ in range(5):
+        with tm:
+            e3.sign(s3, d_msgs, offs3, mlens, keys3, stream=spp)
+    with tc:
+        e3.set_secret_keys(sk3, stream=spp)
+    torch.cuda.synchronize()
+    att3, _ = e3.last_work()
+    ms3, cms = tm.total_ms() / 5, tc.total_ms()
+    ev3 = Engine(3, nk, nm)
+    ev3.set_public_keys(pk3, stream=spp)
+    r3 = torch.empty(nm, dtype=torch.int32, device=dev)
+    ev3.verify(r3, s3, d_msgs, offs3, mlens, keys3, stream=spp)
+    torch.cuda.synchronize()
+    out["d3_sign_16384_loguniform"] = {
+        "sign_per_s_resident_keys": nm / (ms3 / 1e3), "ms_per_batch": ms3, "cache_build_ms_1024_keys": cms,
+        "sign_per_s_incl_cache_build": nm / ((ms3 + cms) / 1e3), "attempts_per_signature": att3 / nm,
+        "mean_mlen": float(mlens.mean()), "all_verified": int((r3 != 0).sum().item()) == 0}
+    del e3, ev3, d_msgs
+
+    # config 4: Dilithium5 verification of 65536 signatures (256 keys x 256 64-byte messages, 10% flipped)
+    d5 = cd.Dilithium(5)
+    p5 = d5.params
+    nk, nm = 256, 65536
+    pool, kpp = alloc_pool(d5.keypair_row_bytes(), nk)
+    pk5 = torch.empty(nk * p5.pk_bytes, dtype=torch.uint8, device=dev)
+    sk5 = torch.empty(nk * p5.sk_bytes, dtype=torch.uint8, device=dev)
+    lib.cudil_keypair_dev(5, pk5.data_ptr(), sk5.data_ptr(), None, pool.data_ptr(), kpp, nk, spp, 0)
+    del pool
+    keys5 = (np.arange(nm) // 256).astype(np.uint32)
+    m5 = torch.randint(0, 256, (nm * 64,), dtype=torch.uint8, device=dev)
+    offs5, lens5 = np.arange(nm, dtype=np.uint64) * 64, np.full(nm, 64, np.uint32)
+    e5 = Engine(5, nk, nm)
+    e5.set_secret_keys(sk5, stream=spp)
+    s5 = torch.empty(nm * p5.sig_bytes, dtype=torch.uint8, device=dev)
+    e5.sign(s5, m5, offs5, lens5, keys5, stream=spp)
+    torch.cuda.synchronize()
+    del e5
+    flip = rng.permutation(nm)[: nm // 10]
+    pos = rng.integers(0, p5.sig_bytes, flip.size)
+    bit = rng.integers(0, 8, flip.size)
+    sv = s5.view(nm, p5.sig_bytes)
+    idx_r = torch.from_numpy(flip).to(dev)
+    idx_c = torch.from_numpy(pos).to(dev)
+    sv[idx_r, idx_c] ^= torch.from_numpy((1 << bit).astype(np.uint8)).to(dev)
+    expect_bad = np.zeros(nm, bool)
+    expect_bad[flip] = True
+    ev5 = Engine(5, nk, nm)
+    ev5.set_public_keys(pk5, stream=spp)
+    r5 = torch.empty(nm, dtype=torch.int32, device=dev)
+    for _ in range(3):
+        ev5.verify(r5, s5, m5, offs5, lens5, keys5, stream=spp)
+    torch.cuda.synchronize()
+    tm = Timer(torch, st)
+    for _ in range(5):
+        with tm:
+            ev5.verify(r5, s5, m5, offs5, lens5, keys5, stream=spp)
+    torch.cuda.synchronize()
+    fused_ms = tm.total_ms() / 5
+    got_bad = (r5.cpu().numpy() != 0)
+    # plain path on the same signatures (per-signature ExpandA and H(pk)); keys expanded per row
+    pk_rows = pk5.view(nk, p5.pk_bytes)[torch.from_numpy(keys5.astype(np.int64)).to(dev)].reshape(-1).contiguous()
+    v_pool, vp = alloc_pool(d5.verify_row_bytes(64), nm)
+    r5p = torch.empty(nm, dtype=torch.int32, device=dev)
+
+    def plain5():
+        lib.cudil_verify_dev(5, r5p.data_ptr(), s5.data_ptr(), p5.sig_bytes, p5.sig_bytes, m5.data_ptr(), 64, 64,
+                             pk_rows.data_ptr(), v_pool.data_ptr(), vp, nm, spp)
+
+    plain5()
+    torch.cuda.synchronize()
+    tm = Timer(torch, st)
+    for _ in range(3):
+        with tm:
+            plain5()
+    torch.cuda.synchronize()
+    plain_ms = tm.total_ms() / 3
+    out["d5_verify_65536_cached_keys"] = {
+        "verify_per_s_fused": nm / (fused_ms / 1e3), "verify_per_s_plain": nm / (plain_ms / 1e3),
+        "speedup": plain_ms / fused_ms, "rejections_exact": bool(np.array_equal(got_bad, expect_bad)),
+        "fused_equals_plain": bool(torch.equal(r5, r5p)), "flipped": int(flip.size)}
+    del v_pool, ev5
+    torch.cuda.empty_cache()
+    return out
 
 
 def ctypes_byref(x):
@@ -394,7 +649,10 @@ def main():
     ap.add_argument("--impl", choices=["cudil", "reference"], default="cudil")
     ap.add_argument("--mode", type=int, default=2, choices=[2, 3, 5])
     ap.add_argument("--batch", type=int, default=10000)
-    ap.add_argument("--threshold", type=int, default=16384, help="exec slots per rejection round (plain path)")
+    ap.add_argument("--thresholds", type=int, nargs="+", default=[4096, 8192, 16384, 32768],
+                    help="exec-slot counts tried for the plain path (the fastest is used)")
+    ap.add_argument("--engine-threads", type=int, default=0, help="fused engine block size (0 = tuned default)")
+    ap.add_argument("--quick", action="store_true", help="headline only (skip configs 1-4)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-sample", type=int, default=4000)
     ap.add_argument("--no-cpu", action="store_true")

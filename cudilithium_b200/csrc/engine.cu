@@ -109,6 +109,13 @@ int cudil_engine_last_status(const cudil_engine *e, unsigned long long *attempts
     return s->error ? CUDIL_ERR_TIMEOUT : CUDIL_OK;
 }
 
+int cudil_engine_last_work(const cudil_engine *e, unsigned long long *attempts, unsigned long long *reject_intt) {
+    if (!e || !e->impl) return CUDIL_ERR_INVALID;
+    if (attempts) *attempts = e->impl->h_status->attempts;
+    if (reject_intt) *reject_intt = e->impl->h_status->intt;
+    return CUDIL_OK;
+}
+
 int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks) {
     if (!e || !e->impl) return CUDIL_ERR_INVALID;
     if (mode) *mode = e->impl->mode;

@@ -65,6 +65,7 @@ struct FusedQueue {
     unsigned long long attempts;
     unsigned int n;            // items in the current batch
     unsigned int pad;
+    unsigned long long intt;   // inverse NTTs run by the rejection checks (for work accounting)
 };
 
 // ------------------------------------------------------------------ cache builders
@@ -220,6 +221,7 @@ static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *loc
         q->done_items = 0;
         q->error = 0;
         q->attempts = 0;
+        q->intt = 0;
     }
 }
 
@@ -429,6 +431,7 @@ __global__ void __launch_bounds__(THREADS) k_fused_sign(const uint8_t *cache, si
                 challenge_strided(ch, masks, g.t);
                 ntt16(ch, g.sm, g.gmask, g.t);
                 bool rejected = false;
+                int n_intt = 0;
                 const int32_t *s1 = reinterpret_cast<const int32_t *>(row + C::SK_S1);
 #pragma unroll 1
                 for (int j = 0; j < L && !rejected; ++j) {
@@ -437,6 +440,7 @@ __global__ void __launch_bounds__(THREADS) k_fused_sign(const uint8_t *cache, si
 #pragma unroll
                     for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
                     intt16(x, g.sm, g.gmask, g.t);
+                    ++n_intt;
                     unpack_z_strided<MODE>(y, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
                     bool bad = false;
 #pragma unroll
@@ -457,7 +461,10 @@ __global__ void __launch_bounds__(THREADS) k_fused_sign(const uint8_t *cache, si
                                                                           g.t * 2 * PM::Z_BITS),
                                              v);
                 }
-                if (rejected) continue;
+                if (rejected) {
+                    if (g.t == 0) atomicAdd(&q->intt, (unsigned long long)n_intt);
+                    continue;
+                }
                 const int32_t *s2 = reinterpret_cast<const int32_t *>(row + C::SK_S2);
                 const int32_t *t0 = reinterpret_cast<const int32_t *>(row + C::SK_T0);
                 uint8_t *hs = slot + C::SL_SIG + PM::SIG_H;
@@ -469,6 +476,7 @@ __global__ void __launch_bounds__(THREADS) k_fused_sign(const uint8_t *cache, si
 #pragma unroll
                     for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
                     intt16(x, g.sm, g.gmask, g.t);
+                    ++n_intt;
                     const int32_t *w0 = reinterpret_cast<const int32_t *>(slot + C::SL_W0) + (size_t)i * N;
                     bool bad = false;
 #pragma unroll
@@ -484,6 +492,7 @@ __global__ void __launch_bounds__(THREADS) k_fused_sign(const uint8_t *cache, si
 #pragma unroll
                     for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
                     intt16(x, g.sm, g.gmask, g.t);
+                    ++n_intt;
 #pragma unroll
                     for (int m = 0; m < 16; ++m) {
                         x[m] = reduce32(x[m]);
@@ -511,6 +520,7 @@ __global__ void __launch_bounds__(THREADS) k_fused_sign(const uint8_t *cache, si
                     }
                     if (g.t == 0) hs[OMEGA + i] = (uint8_t)cnt;
                 }
+                if (g.t == 0) atomicAdd(&q->intt, (unsigned long long)n_intt);
                 if (rejected) continue;
                 for (int qq = cnt + g.t; qq < OMEGA; qq += 16) hs[qq] = 0;
                 __syncwarp(g.gmask);

@@ -96,6 +96,12 @@ class Engine:
         check(rc, "engine batch")
         return a.value, e.value
 
+    def last_work(self) -> tuple[int, int]:
+        """(attempts, inverse NTTs of the rejection checks) of the last signing batch."""
+        a, i = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        lib.cudil_engine_last_work(self.h, ctypes.byref(a), ctypes.byref(i))
+        return a.value, i.value
+
     # ---- numpy conveniences (synchronous)
     def sign_np(self, msgs, key_idx) -> np.ndarray:
         d_msgs, offs, lens = pack_messages(msgs)

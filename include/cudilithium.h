@@ -164,6 +164,9 @@ int cudil_engine_verify(cudil_engine *e, int *d_ret, const uint8_t *d_sig, const
                         const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
                         void *stream);
 int cudil_engine_last_status(const cudil_engine *e, unsigned long long *attempts, unsigned *error);
+/* Work counters of the last completed signing batch: attempts run and inverse NTTs executed by the
+ * rejection checks (for throughput accounting). */
+int cudil_engine_last_work(const cudil_engine *e, unsigned long long *attempts, unsigned long long *reject_intt);
 int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks);
 
 /* Peak of the 32-bit LOP3/funnel-shift mix Keccak-f[1600] issues: launches `blocks` x 256 threads
