@@ -1,0 +1,110 @@
+"""Autotuner for the fused engine: picks the block size and the signer's per-block speculation
+target for each parameter set by timing real signing batches, and caches the result as JSON
+(``cudilithium_b200/tuned.json``, keyed by GPU name).
+
+    python -m cudilithium_b200.autotune [--modes 2 3 5] [--batch 16384]
+
+``Engine(..., threads=0)`` and ``tuned(mode)`` read the cache; without an entry for this GPU
+the built-in defaults below apply.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from pathlib import Path
+
+TUNED_PATH = Path(__file__).resolve().parent / "tuned.json"
+# measured on B200 (Dilithium2, 10000 and 65536 single-use keys): 256 threads per block and a
+# per-block target of 32 attempts in flight gave the highest signing throughput
+DEFAULTS = {2: {"threads": 256, "spec_slots": 32}, 3: {"threads": 256, "spec_slots": 32},
+            5: {"threads": 256, "spec_slots": 32}}
+THREADS = (128, 256)
+SPEC = (16, 32, 64, 128)
+
+
+def _gpu_name() -> str:
+    import torch
+    return torch.cuda.get_device_name(torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
+
+
+def tuned(mode: int) -> dict:
+    """Tuned engine settings for this GPU (falls back to DEFAULTS)."""
+    try:
+        data = json.loads(TUNED_PATH.read_text())
+        return data.get(_gpu_name(), {}).get(str(mode), DEFAULTS[mode])
+    except (OSError, ValueError):
+        return DEFAULTS[mode]
+
+
+def tune_mode(mode: int, batch: int, reps: int = 3) -> dict:
+    import numpy as np
+    import torch
+
+    import cudilithium_b200 as cd
+    from cudilithium_b200.api import alloc_pool
+    from cudilithium_b200.engine import Engine
+    lib = cd.lib
+    d = cd.Dilithium(mode)
+    pm = d.params
+    dev = torch.device("cuda")
+    spp = torch.cuda.current_stream().cuda_stream
+    pool, kpp = alloc_pool(d.keypair_row_bytes(), batch)
+    pk = torch.empty(batch * pm.pk_bytes, dtype=torch.uint8, device=dev)
+    sk = torch.empty(batch * pm.sk_bytes, dtype=torch.uint8, device=dev)
+    lib.cudil_keypair_dev(mode, pk.data_ptr(), sk.data_ptr(), None, pool.data_ptr(), kpp, batch, spp, 0)
+    del pool
+    m = torch.randint(0, 256, (batch * 32,), dtype=torch.uint8, device=dev)
+    offs = np.arange(batch, dtype=np.uint64) * 32
+    lens = np.full(batch, 32, np.uint32)
+    keys = np.arange(batch, dtype=np.uint32)
+    sig = torch.empty(batch * pm.sig_bytes, dtype=torch.uint8, device=dev)
+    results = []
+    ref = None
+    for t in THREADS:
+        e = Engine(mode, batch, batch, threads=t)
+        e.set_secret_keys(sk, stream=spp)
+        for s in SPEC:
+            e.set_spec_slots(s)
+            e.sign(sig, m, offs, lens, keys, stream=spp)
+            torch.cuda.synchronize()
+            if ref is None:
+                ref = sig.clone()
+            assert torch.equal(sig, ref), "tuning candidates disagree"
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                e.sign(sig, m, offs, lens, keys, stream=spp)
+            b.record()
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b) / reps
+            results.append({"threads": t, "spec_slots": s, "ms": ms, "sign_per_s": batch / (ms / 1e3)})
+        e.close()
+    best = min(results, key=lambda r: r["ms"])
+    return {"threads": best["threads"], "spec_slots": best["spec_slots"], "batch": batch,
+            "sign_per_s": best["sign_per_s"], "candidates": results, "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--modes", type=int, nargs="+", default=[2, 3, 5])
+    ap.add_argument("--batch", type=int, default=16384)
+    args = ap.parse_args()
+    name = _gpu_name()
+    data = {}
+    if TUNED_PATH.exists():
+        try:
+            data = json.loads(TUNED_PATH.read_text())
+        except ValueError:
+            data = {}
+    entry = data.setdefault(name, {})
+    for mode in args.modes:
+        r = tune_mode(mode, args.batch)
+        entry[str(mode)] = r
+        print(json.dumps({"mode": mode, "threads": r["threads"], "spec_slots": r["spec_slots"],
+                          "sign_per_s": round(r["sign_per_s"])}), flush=True)
+    TUNED_PATH.write_text(json.dumps(data, indent=1))
+
+
+if __name__ == "__main__":
+    main()

@@ -26,7 +26,8 @@ struct EngineBase {
     uint8_t *sk_cache = nullptr, *pk_cache = nullptr;
     size_t sk_pitch = 0, pk_pitch = 0;
     uint8_t *items = nullptr;       // max_items * 128
-    unsigned *best = nullptr, *locks = nullptr;
+    unsigned *best = nullptr, *locks = nullptr, *next_nonce = nullptr, *inflight = nullptr;
+    unsigned spec_slots = 0;  // signer's target of attempts in flight (0 = default for the grid)
     FusedQueue *q = nullptr;
     // metadata (device) and its pinned staging
     unsigned *d_key = nullptr, *d_mlen = nullptr, *d_order = nullptr;
@@ -63,9 +64,9 @@ struct EngineImpl : EngineBase {
 
     // Device bytes the engine needs (the admission budget checks this before allocating).
     static size_t required_bytes(size_t max_keys, size_t max_items, int threads, int sign_grid, int verify_grid) {
-        return max_keys * (align256(C::SK_ROW) + align256(C::PK_ROW)) + max_items * (C::ITEM_BYTES + 2 * sizeof(unsigned)) +
+        return max_keys * (align256(C::SK_ROW) + align256(C::PK_ROW)) + max_items * (C::ITEM_BYTES + 4 * sizeof(unsigned)) +
                stage_bytes(max_items) + sizeof(FusedQueue) +
-               std::max((size_t)sign_grid * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
+               std::max((size_t)sign_grid * 2 * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
     }
 
     template <int T>
@@ -95,10 +96,13 @@ struct EngineImpl : EngineBase {
         if (budget && device_bytes > budget) return CUDIL_ERR_BUDGET;
         sk_pitch = align256(C::SK_ROW);
         pk_pitch = align256(C::PK_ROW);
-        scratch_bytes = std::max((size_t)sign_grid * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
+        scratch_bytes = std::max((size_t)sign_grid * 2 * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
+        spec_slots = (unsigned)threads;
         if (cudaMalloc(&sk_cache, mk * sk_pitch) != cudaSuccess || cudaMalloc(&pk_cache, mk * pk_pitch) != cudaSuccess ||
             cudaMalloc(&items, mi * C::ITEM_BYTES) != cudaSuccess || cudaMalloc(&best, mi * sizeof(unsigned)) != cudaSuccess ||
             cudaMalloc(&locks, mi * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&q, sizeof(FusedQueue)) != cudaSuccess ||
+            cudaMalloc(&next_nonce, mi * sizeof(unsigned)) != cudaSuccess ||
+            cudaMalloc(&inflight, mi * sizeof(unsigned)) != cudaSuccess ||
             cudaMalloc(&d_key, mi * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&d_mlen, mi * sizeof(unsigned)) != cudaSuccess ||
             cudaMalloc(&d_order, mi * sizeof(unsigned)) != cudaSuccess ||
             cudaMalloc(&d_off, mi * sizeof(unsigned long long)) != cudaSuccess || cudaMalloc(&scratch, scratch_bytes) != cudaSuccess ||
@@ -116,6 +120,8 @@ struct EngineImpl : EngineBase {
         cudaFree(items);
         cudaFree(best);
         cudaFree(locks);
+        cudaFree(next_nonce);
+        cudaFree(inflight);
         cudaFree(q);
         cudaFree(d_key);
         cudaFree(d_mlen);
@@ -189,17 +195,18 @@ struct EngineImpl : EngineBase {
     template <int T>
     void record_sign(cudaStream_t st, uint8_t *d_sig, const uint8_t *d_msgs) {
         MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order};
-        k_fused_init<<<std::max(1, sm_count * 2), 256, 0, st>>>(q, best, locks);
+        k_fused_init<<<std::max(1, sm_count * 2), 256, 0, st>>>(q, best, locks, next_nonce, inflight);
         k_fused_prehash<MODE><<<prehash_grid, kBlock, 0, st>>>(sk_cache, sk_pitch, mr, items, q);
-        k_fused_sign<MODE, T><<<sign_grid, T, sign_smem, st>>>(sk_cache, sk_pitch, d_key, items, d_sig, PM::SIG_BYTES, scratch, q,
-                                                              best, locks);
+        FusedSignArgs a{sk_cache, sk_pitch, d_key, items, d_sig, (size_t)PM::SIG_BYTES, scratch, q, best, locks, next_nonce,
+                        inflight, spec_slots};
+        k_fused_sign<MODE, T><<<sign_grid, T, sign_smem, st>>>(a);
         cudaMemcpyAsync(h_status, q, sizeof(FusedQueue), cudaMemcpyDeviceToHost, st);
     }
 
     template <int T>
     void record_verify(cudaStream_t st, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs) {
         MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order};
-        k_fused_init<<<1, 32, 0, st>>>(q, best, locks);
+        k_fused_init<<<1, 32, 0, st>>>(q, best, locks, nullptr, nullptr);
         k_fused_verify<MODE, T><<<verify_grid, T, verify_smem, st>>>(pk_cache, pk_pitch, mr, d_sig, PM::SIG_BYTES, d_ret,
                                                                     scratch, q);
         cudaMemcpyAsync(h_status, q, sizeof(FusedQueue), cudaMemcpyDeviceToHost, st);
@@ -278,6 +285,13 @@ struct EngineImpl : EngineBase {
     }
 
     const uint8_t *g_verify_msgs = nullptr;
+
+    // Target of signing attempts in flight; the graph is re-captured on the next batch.
+    int set_spec_slots(unsigned v) {
+        spec_slots = v ? std::min<unsigned>(v, 2u * (unsigned)threads) : (unsigned)threads;
+        g_sign_key[0] = nullptr;
+        return CUDIL_OK;
+    }
 };
 
 }  // namespace cudil

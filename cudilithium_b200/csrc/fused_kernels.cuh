@@ -66,6 +66,8 @@ struct FusedQueue {
     unsigned int n;            // items in the current batch
     unsigned int pad;
     unsigned long long intt;   // inverse NTTs run by the rejection checks (for work accounting)
+    unsigned int rr;           // round-robin probe position of the signer's work queue
+    unsigned int pad2;
 };
 
 // ------------------------------------------------------------------ cache builders
@@ -210,11 +212,14 @@ __global__ void __launch_bounds__(kBlock) k_fused_prehash(const uint8_t *cache, 
 }
 
 // Resets the per-item winner state and the queue for q->n items (n set by the host copy).
-static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *locks) {
+static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *locks, unsigned *next_nonce,
+                                    unsigned *inflight) {
     const unsigned n = q->n;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         best[i] = 0xFFFFFFFFu;
         locks[i] = 0u;
+        if (next_nonce) next_nonce[i] = 0u;
+        if (inflight) inflight[i] = 0u;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         q->next_ticket = 0;
@@ -222,344 +227,391 @@ static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *loc
         q->error = 0;
         q->attempts = 0;
         q->intt = 0;
+        q->rr = 0;
     }
 }
 
 // ------------------------------------------------------------------ persistent signer
+//
+// Work queue.  Block b owns the items b, b + grid, b + 2*grid, ... and schedules them itself, so
+// refilling slots touches no shared counter.  Every owned item has a next-nonce counter and an
+// in-flight counter; a claim gives pending items (no accepted nonce yet) their next nonce, at most
+// D in flight per item.  D = 2 while the block has many pending items (one attempt being checked,
+// the next one already being computed) and grows up to 64 as its pending items run out, so the last
+// items of a block are speculated deeply instead of taking one rejection round after another.
+// Nonces of an item are issued in increasing order and every issued attempt completes before the
+// block exits, so the winner -- the smallest accepted nonce -- is the deterministic signature.
+//
+struct FusedSignArgs {
+    const uint8_t *cache;
+    size_t cpitch;
+    const unsigned *key_idx;
+    const uint8_t *items;
+    uint8_t *sig_out;
+    size_t sig_pitch;
+    uint8_t *scratch;
+    FusedQueue *q;
+    unsigned *best, *locks, *next_nonce, *inflight;
+    unsigned spec_slots;  // per-block target of attempts in flight (<= 2 * THREADS)
+};
 
 template <int MODE, int THREADS>
 struct FusedSignSmem {
     using PM = P<MODE>;
     static constexpr int G = THREADS / 16;
-    static constexpr size_t CTRL = 4096;
-    static constexpr size_t PH_W = (size_t)G * (PM::L * N * 4 + NTT_SMEM_WORDS * 4);
-    static constexpr size_t PH_C = (size_t)THREADS * (SHAKE256_RATE + 64);
-    static constexpr size_t BYTES = CTRL + (PH_W > PH_C ? PH_W : PH_C);
+    static constexpr size_t CTRL = 4 * THREADS * sizeof(unsigned) + 256;
+    static constexpr size_t PH_N = (size_t)G * (PM::L * N * 4 + NTT_SMEM_WORDS * 4);
+    static constexpr size_t PH_K = (size_t)THREADS * (34 + 16) * 4;
+    static constexpr size_t BYTES = CTRL + (PH_N > PH_K ? PH_N : PH_K);
 };
 
 constexpr unsigned kLockSpinLimit = 1u << 22;
 
 template <int MODE, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_fused_sign(const uint8_t *cache, size_t cpitch, const unsigned *key_idx,
-                                                        const uint8_t *items, uint8_t *sig_out, size_t sig_pitch,
-                                                        uint8_t *scratch, FusedQueue *q, unsigned *best,
-                                                        unsigned *locks) {
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSignArgs arg) {
     using PM = P<MODE>;
     using C = Cache<MODE>;
-    constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA, A = THREADS;
-    constexpr int G = THREADS / 16;
+    constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA, A = THREADS, G = THREADS / 16;
+    enum { CT_PEND = 0, CT_KJOB, CT_NJOB, CT_NA0, CT_NA1, CT_EXIT };
     extern __shared__ __align__(16) uint8_t fs_smem[];
-    unsigned *s_item = reinterpret_cast<unsigned *>(fs_smem);          // [A]
-    unsigned *s_nonce = s_item + A;                                      // [A]
-    unsigned *s_ctl = s_nonce + A;                                       // [8]
-    uint8_t *ph = fs_smem + FusedSignSmem<MODE, THREADS>::CTRL;         // phase-shared region
-    const int tid = threadIdx.x, gi = tid >> 4, lane = tid & 31;
+    unsigned *s_item = reinterpret_cast<unsigned *>(fs_smem);   // [2][A]
+    unsigned *s_nonce = s_item + 2 * A;                          // [2][A]
+    unsigned *s_ctl = s_nonce + 2 * A;                           // CT_* and per-warp counts
+    uint8_t *ph = fs_smem + FusedSignSmem<MODE, THREADS>::CTRL;
+    FusedQueue *q = arg.q;
+    const int tid = threadIdx.x, gi = tid >> 4, lane = tid & 31, lane_off = lane & 16;
     const unsigned n = q->n;
-    const unsigned long long total = (unsigned long long)n * 65536ull;  // nonce is 16-bit
-    uint8_t *my_slots = scratch + (size_t)blockIdx.x * A * C::SLOT;
+    uint8_t *my_slots = arg.scratch + (size_t)blockIdx.x * 2 * A * C::SLOT;
+    auto slot_of = [&](int buf, int a) { return my_slots + ((size_t)buf * A + a) * C::SLOT; };
 
-    for (;;) {
-        // ---------------- claim up to A live attempts from the ticket queue
-        if (tid == 0) s_ctl[0] = 0;  // filled
+    Group g;
+    g.t = tid & 15;
+    g.gmask = 0xFFFFu << lane_off;
+
+    // ---------------- claim: fill batch `buf` with up to A attempts of this block's items
+    // (block-collective; warp 0 scans the owned items, one item per lane per pass)
+    const unsigned grid = gridDim.x, b0 = blockIdx.x;
+    const unsigned n_own = (b0 < n) ? (n - b0 + grid - 1) / grid : 0u;
+    auto claim = [&](int buf) {
+        if (tid < 32) {
+            const unsigned pend = s_ctl[CT_PEND];
+            unsigned D = 0;
+            if (pend) {
+                const unsigned t = arg.spec_slots / pend;
+                D = t < 2u ? 2u : (t > 64u ? 64u : t);
+            }
+            unsigned filled = 0;
+#pragma unroll 1
+            for (unsigned pass = 0; pass < D && filled < (unsigned)A; ++pass) {
+#pragma unroll 1
+                for (unsigned k0 = 0; k0 < n_own && filled < (unsigned)A; k0 += 32) {
+                    const unsigned k = k0 + lane, i = b0 + k * grid;
+                    bool ok = false;
+                    if (k < n_own && __ldcg(arg.best + i) == 0xFFFFFFFFu && __ldcg(arg.inflight + i) <= pass) ok = true;
+                    const unsigned bal = __ballot_sync(0xFFFFFFFFu, ok);
+                    const unsigned pos = filled + __popc(bal & ((1u << lane) - 1u));
+                    if (ok && pos < (unsigned)A) {
+                        const unsigned nn = atomicAdd(arg.next_nonce + i, 1u);
+                        if (nn < 65536u) {
+                            atomicAdd(arg.inflight + i, 1u);
+                            s_item[buf * A + pos] = i;
+                            s_nonce[buf * A + pos] = nn;
+                        } else {
+                            // 2^16 attempts without acceptance: never happens in practice; mark the
+                            // slot as a no-op by reusing the item with an out-of-range nonce
+                            s_item[buf * A + pos] = i;
+                            s_nonce[buf * A + pos] = 0xFFFFFFFFu;
+                            atomicAdd(arg.inflight + i, 1u);
+                        }
+                    }
+                    filled += __popc(bal);
+                    if (filled > (unsigned)A) filled = A;
+                }
+            }
+            if (lane == 0) {
+                s_ctl[CT_NA0 + buf] = filled;
+                s_ctl[CT_KJOB] = 0;
+                s_ctl[CT_NJOB] = 0;
+                if (filled) atomicAdd(&q->attempts, (unsigned long long)filled);
+            }
+        }
         __syncthreads();
+    };
+
+    // ---------------- Keccak phase: challenge of batch cb (jobs < na_c), ExpandMask of batch nb
+    auto keccak_phase = [&](int cb, int na_c, int nb, int na_n) {
+        uint32_t *blkw = reinterpret_cast<uint32_t *>(ph) + tid;
+        uint32_t *mask = reinterpret_cast<uint32_t *>(ph) + 34 * THREADS + tid;
+        const int total = na_c + na_n * L;
+#pragma unroll 1
         for (;;) {
-            if (tid == 0) {
-                const unsigned filled = s_ctl[0];
-                const unsigned done = *reinterpret_cast<volatile unsigned *>(&q->done_items);
-                unsigned need = (done >= n) ? 0u : (unsigned)A - filled;
-                unsigned long long base = 0;
-                if (need) {
-                    base = atomicAdd(&q->next_ticket, (unsigned long long)need);
-                    if (base >= total) need = 0;
-                }
-                s_ctl[1] = need;
-                s_ctl[2] = (unsigned)(base & 0xFFFFFFFFull);
-                s_ctl[3] = (unsigned)(base >> 32);
+            const int job = (int)atomicAdd(&s_ctl[CT_KJOB], 1u);
+            if (job >= total) break;
+            if (job < na_c) {
+                const unsigned item = s_item[cb * A + job];
+                uint8_t *slot = slot_of(cb, job);
+                uint32_t al[25], ah[25];
+                TwoPart src{arg.items + (size_t)item * C::ITEM_BYTES, 8, slot + C::SL_W1P, PM::W1PACKED_BYTES};
+                shake_absorb<SHAKE256_RATE>(al, ah, src, CRHBYTES + PM::W1PACKED_BYTES);
+                keccak_f1600(al, ah);
+                uint2 ct[4];
+#pragma unroll
+                for (int w = 0; w < 4; ++w) ct[w] = make_uint2(al[w], ah[w]);
+                uint2 *sg = reinterpret_cast<uint2 *>(slot + C::SL_SIG);
+#pragma unroll
+                for (int w = 0; w < 4; ++w) sg[w] = ct[w];
+                sample_in_ball<PM::TAU, THREADS>(ct, blkw, mask);
+                uint4 *mo = reinterpret_cast<uint4 *>(slot + C::SL_CM);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    mo[k] = make_uint4(mask[(4 * k) * THREADS], mask[(4 * k + 1) * THREADS], mask[(4 * k + 2) * THREADS],
+                                       mask[(4 * k + 3) * THREADS]);
+            } else {
+                const int idx = job - na_c, a = idx / L, j = idx % L;
+                const unsigned item = s_item[nb * A + a], nonce = s_nonce[nb * A + a];
+                uint2 rhop[8];
+                ld_lanes(rhop, arg.items + (size_t)item * C::ITEM_BYTES + 64);
+                expand_mask_stream<MODE>(slot_of(nb, a) + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, rhop,
+                                         (uint32_t)(L * nonce + j));
             }
-            __syncthreads();
-            const unsigned need = s_ctl[1];
-            if (need == 0) break;
-            const unsigned long long t = ((unsigned long long)s_ctl[3] << 32 | s_ctl[2]) + (unsigned)tid;
-            bool live = false;
-            unsigned item = 0, nonce = 0;
-            if ((unsigned)tid < need && t < total) {
-                item = (unsigned)(t % n);
-                nonce = (unsigned)(t / n);
-                live = __ldcg(best + item) > nonce;
-            }
-            // block-wide compaction of the live tickets into the slot list
-            const unsigned bal = __ballot_sync(0xFFFFFFFFu, live);
-            if (lane == 0) s_ctl[4 + 0] = 0;  // placeholder (warp offsets computed below)
-            __shared__ unsigned s_wcnt[THREADS / 32];
-            if (lane == 0) s_wcnt[tid >> 5] = __popc(bal);
-            __syncthreads();
-            unsigned off = s_ctl[0];
-            for (int w = 0; w < (tid >> 5); ++w) off += s_wcnt[w];
-            if (live) {
-                const unsigned pos = off + __popc(bal & ((1u << lane) - 1u));
-                s_item[pos] = item;
-                s_nonce[pos] = nonce;
-            }
-            __syncthreads();
-            if (tid == 0) {
-                unsigned tot = 0;
-                for (int w = 0; w < THREADS / 32; ++w) tot += s_wcnt[w];
-                s_ctl[0] += tot;
-            }
-            __syncthreads();
-            if (s_ctl[0] >= (unsigned)A) break;
         }
-        const int na = (int)s_ctl[0];
-        if (na == 0) break;
-        if (tid == 0) atomicAdd(&q->attempts, (unsigned long long)na);
+    };
 
-        // ---------------- ExpandMask: one thread per attempt, L streams each
-        if (tid < na) {
-            const unsigned item = s_item[tid], nonce = s_nonce[tid];
-            uint2 rhop[8];
-            ld_lanes(rhop, items + (size_t)item * C::ITEM_BYTES + 64);
-            uint8_t *slot = my_slots + (size_t)tid * C::SLOT;
-#pragma unroll 1
-            for (int j = 0; j < L; ++j)
-                expand_mask_stream<MODE>(slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, rhop, (uint32_t)(L * nonce + j));
+    // rejection checks, hints and publication of one attempt (group-collective)
+    auto reject_job = [&](int cb, int a) {
+        const unsigned item = s_item[cb * A + a], nonce = s_nonce[cb * A + a];
+        if (nonce > 0xFFFFu) {
+            if (g.t == 0) atomicSub(arg.inflight + item, 1u);
+            return;
         }
-        __syncthreads();
-
-        // ---------------- w = invNTT(A_hat * NTT(y)), Decompose: one group per attempt
+        uint8_t *slot = slot_of(cb, a);
+        const uint8_t *row = arg.cache + (size_t)arg.key_idx[item] * arg.cpitch;
+        g.sm = reinterpret_cast<int32_t *>(ph) + (size_t)gi * (L * N + NTT_SMEM_WORDS) + L * N;
+        uint32_t masks[16];
         {
-            int32_t *yh = reinterpret_cast<int32_t *>(ph) + (size_t)gi * (L * N + NTT_SMEM_WORDS);
-            Group g;
-            g.t = tid & 15;
-            g.gmask = 0xFFFFu << (lane & 16);
-            g.sm = yh + L * N;
-            for (int a = gi; a < na; a += G) {
-                uint8_t *slot = my_slots + (size_t)a * C::SLOT;
-                const uint8_t *row = cache + (size_t)key_idx[s_item[a]] * cpitch;
-#pragma unroll 1
-                for (int j = 0; j < L; ++j) {
-                    int32_t x[16];
-                    unpack_z_strided<MODE>(x, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
-                    ntt16(x, g.sm, g.gmask, g.t);
-                    store16_contig(yh + j * N + 16 * g.t, x);
-                }
-                __syncwarp(g.gmask);
-#pragma unroll 1
-                for (int i = 0; i < K; ++i) {
-                    const int32_t *mat = reinterpret_cast<const int32_t *>(row + C::SK_MAT) + (size_t)i * L * N;
-                    int32_t acc[16];
+            const uint4 *mi = reinterpret_cast<const uint4 *>(slot + C::SL_CM);
 #pragma unroll
-                    for (int m = 0; m < 16; ++m) acc[m] = 0;
-#pragma unroll
-                    for (int j = 0; j < L; ++j) {
-                        int32_t av[16], yv[16];
-                        load16_contig(av, mat + (size_t)j * N + 16 * g.t);
-                        load16_contig(yv, yh + j * N + 16 * g.t);
-#pragma unroll
-                        for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], yv[m]);
-                    }
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m]);
-                    intt16(acc, g.sm, g.gmask, g.t);
-                    int32_t *w0 = reinterpret_cast<int32_t *>(slot + C::SL_W0) + (size_t)i * N;
-                    int32_t w1[16];
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) {
-                        int32_t a0;
-                        w1[m] = decompose<MODE>(a0, caddq(acc[m]));
-                        w0[g.t + 16 * m] = a0;
-                    }
-                    int32_t w1c[16];
-                    strided_to_contig(g, w1, w1c);
-                    uint32_t v[16];
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) v[m] = (uint32_t)w1c[m];
-                    pack16_words<PM::W1_BITS>(
-                        reinterpret_cast<uint32_t *>(slot + C::SL_W1P + (size_t)i * PM::POLYW1_PACKED + g.t * 2 * PM::W1_BITS), v);
-                }
-                __syncwarp(g.gmask);
+            for (int k = 0; k < 4; ++k) {
+                const uint4 v = mi[k];
+                masks[4 * k] = v.x;
+                masks[4 * k + 1] = v.y;
+                masks[4 * k + 2] = v.z;
+                masks[4 * k + 3] = v.w;
             }
         }
-        __syncthreads();
-
-        // ---------------- challenge: one thread per attempt
-        if (tid < na) {
-            const unsigned item = s_item[tid];
-            uint8_t *slot = my_slots + (size_t)tid * C::SLOT;
-            uint32_t al[25], ah[25];
-            TwoPart src{items + (size_t)item * C::ITEM_BYTES, 8, slot + C::SL_W1P, PM::W1PACKED_BYTES};
-            shake_absorb<SHAKE256_RATE>(al, ah, src, CRHBYTES + PM::W1PACKED_BYTES);
-            keccak_f1600(al, ah);
-            uint2 ct[4];
-#pragma unroll
-            for (int w = 0; w < 4; ++w) ct[w] = make_uint2(al[w], ah[w]);
-            uint2 *sg = reinterpret_cast<uint2 *>(slot + C::SL_SIG);
-#pragma unroll
-            for (int w = 0; w < 4; ++w) sg[w] = ct[w];
-            uint8_t *blk = ph + (size_t)tid * SHAKE256_RATE;
-            uint32_t *mask = reinterpret_cast<uint32_t *>(ph + (size_t)THREADS * SHAKE256_RATE) + tid * 16;
-            sample_in_ball<PM::TAU>(ct, blk, mask);
-            uint4 *mo = reinterpret_cast<uint4 *>(slot + C::SL_CM);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) mo[k] = make_uint4(mask[4 * k], mask[4 * k + 1], mask[4 * k + 2], mask[4 * k + 3]);
-        }
-        __syncthreads();
-
-        // ---------------- rejection checks, hints, publication: one group per attempt
-        {
-            Group g;
-            g.t = tid & 15;
-            g.gmask = 0xFFFFu << (lane & 16);
-            g.sm = reinterpret_cast<int32_t *>(ph) + (size_t)gi * NTT_SMEM_WORDS;
-            const int lane_off = lane & 16;
-            for (int a = gi; a < na; a += G) {
-                const unsigned item = s_item[a], nonce = s_nonce[a];
-                uint8_t *slot = my_slots + (size_t)a * C::SLOT;
-                const uint8_t *row = cache + (size_t)key_idx[item] * cpitch;
-                uint32_t masks[16];
-                {
-                    const uint4 *mi = reinterpret_cast<const uint4 *>(slot + C::SL_CM);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const uint4 v = mi[k];
-                        masks[4 * k] = v.x;
-                        masks[4 * k + 1] = v.y;
-                        masks[4 * k + 2] = v.z;
-                        masks[4 * k + 3] = v.w;
-                    }
-                }
-                int32_t ch[16];
-                challenge_strided(ch, masks, g.t);
-                ntt16(ch, g.sm, g.gmask, g.t);
-                bool rejected = false;
-                int n_intt = 0;
-                const int32_t *s1 = reinterpret_cast<const int32_t *>(row + C::SK_S1);
+        int32_t ch[16];
+        challenge_strided(ch, masks, g.t);
+        ntt16(ch, g.sm, g.gmask, g.t);
+        const int32_t *s1 = reinterpret_cast<const int32_t *>(row + C::SK_S1);
+        const int32_t *s2 = reinterpret_cast<const int32_t *>(row + C::SK_S2);
+        const int32_t *t0 = reinterpret_cast<const int32_t *>(row + C::SK_T0);
+        uint8_t *hs = slot + C::SL_SIG + PM::SIG_H;
+        bool rejected = false;
+        int cnt = 0, n_intt = 0;
+        int32_t r0[16];
+        // polynomial steps: z_0..z_{L-1}, then (r0_i, ct0_i) for i < K -- the order of the reference
 #pragma unroll 1
-                for (int j = 0; j < L && !rejected; ++j) {
-                    int32_t x[16], y[16];
-                    load16_contig(x, s1 + (size_t)j * N + 16 * g.t);
+        for (int step = 0; step < L + 2 * K; ++step) {
+            const int i = (step - L) >> 1;
+            const bool is_z = step < L, is_r0 = !is_z && (((step - L) & 1) == 0);
+            const int32_t *src = is_z ? s1 + (size_t)step * N : (is_r0 ? s2 : t0) + (size_t)i * N;
+            int32_t x[16];
+            load16_contig(x, src + 16 * g.t);
 #pragma unroll
-                    for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
-                    intt16(x, g.sm, g.gmask, g.t);
-                    ++n_intt;
-                    unpack_z_strided<MODE>(y, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
-                    bool bad = false;
+            for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
+            intt16(x, g.sm, g.gmask, g.t);
+            ++n_intt;
+            bool bad = false;
+            if (is_z) {
+                int32_t y[16];
+                unpack_z_strided<MODE>(y, slot + C::SL_Y + (size_t)step * PM::POLYZ_PACKED, g.t);
 #pragma unroll
-                    for (int m = 0; m < 16; ++m) {
-                        x[m] = reduce32(x[m] + y[m]);
-                        bad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
-                    }
-                    if (group_any(g, bad)) {
-                        rejected = true;
-                        break;
-                    }
-                    int32_t zc[16];
-                    strided_to_contig(g, x, zc);
-                    uint32_t v[16];
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
-                    pack16_words<PM::Z_BITS>(reinterpret_cast<uint32_t *>(slot + C::SL_SIG + PM::SIG_Z + (size_t)j * PM::POLYZ_PACKED +
-                                                                          g.t * 2 * PM::Z_BITS),
-                                             v);
+                for (int m = 0; m < 16; ++m) {
+                    x[m] = reduce32(x[m] + y[m]);
+                    bad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
                 }
-                if (rejected) {
-                    if (g.t == 0) atomicAdd(&q->intt, (unsigned long long)n_intt);
-                    continue;
+                if (group_any(g, bad)) {
+                    rejected = true;
+                    break;
                 }
-                const int32_t *s2 = reinterpret_cast<const int32_t *>(row + C::SK_S2);
-                const int32_t *t0 = reinterpret_cast<const int32_t *>(row + C::SK_T0);
-                uint8_t *hs = slot + C::SL_SIG + PM::SIG_H;
-                int cnt = 0;
-#pragma unroll 1
-                for (int i = 0; i < K && !rejected; ++i) {
-                    int32_t x[16], r0[16];
-                    load16_contig(x, s2 + (size_t)i * N + 16 * g.t);
+                int32_t zc[16];
+                strided_to_contig(g, x, zc);
+                uint32_t v[16];
 #pragma unroll
-                    for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
-                    intt16(x, g.sm, g.gmask, g.t);
-                    ++n_intt;
-                    const int32_t *w0 = reinterpret_cast<const int32_t *>(slot + C::SL_W0) + (size_t)i * N;
-                    bool bad = false;
+                for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
+                pack16_words<PM::Z_BITS>(
+                    reinterpret_cast<uint32_t *>(slot + C::SL_SIG + PM::SIG_Z + (size_t)step * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
+            } else if (is_r0) {
+                const int32_t *w0 = reinterpret_cast<const int32_t *>(slot + C::SL_W0) + (size_t)i * N;
 #pragma unroll
-                    for (int m = 0; m < 16; ++m) {
-                        r0[m] = reduce32(w0[g.t + 16 * m] - x[m]);
-                        bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
-                    }
-                    if (group_any(g, bad)) {
-                        rejected = true;
-                        break;
-                    }
-                    load16_contig(x, t0 + (size_t)i * N + 16 * g.t);
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
-                    intt16(x, g.sm, g.gmask, g.t);
-                    ++n_intt;
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) {
-                        x[m] = reduce32(x[m]);
-                        bad |= exceeds(x[m], PM::GAMMA2);
-                    }
-                    if (group_any(g, bad)) {
-                        rejected = true;
-                        break;
-                    }
-                    const uint8_t *w1p = slot + C::SL_W1P + (size_t)i * PM::POLYW1_PACKED;
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) {
-                        const int32_t w1 = (int32_t)get_bits(w1p, (g.t + 16 * m) * PM::W1_BITS, PM::W1_BITS);
-                        const unsigned h = make_hint<MODE>(r0[m] + x[m], w1);
-                        const unsigned bal = (__ballot_sync(g.gmask, h) >> lane_off) & 0xFFFFu;
-                        if (h) {
-                            const int idx = cnt + __popc(bal & ((1u << g.t) - 1u));
-                            if (idx < OMEGA) hs[idx] = (uint8_t)(g.t + 16 * m);
-                        }
-                        cnt += __popc(bal);
-                    }
-                    if (cnt > OMEGA) {
-                        rejected = true;
-                        break;
-                    }
-                    if (g.t == 0) hs[OMEGA + i] = (uint8_t)cnt;
+                for (int m = 0; m < 16; ++m) {
+                    r0[m] = reduce32(w0[g.t + 16 * m] - x[m]);
+                    bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
                 }
-                if (g.t == 0) atomicAdd(&q->intt, (unsigned long long)n_intt);
-                if (rejected) continue;
-                for (int qq = cnt + g.t; qq < OMEGA; qq += 16) hs[qq] = 0;
-                __syncwarp(g.gmask);
-                // accepted: lower the item's best nonce; publish if this attempt holds the minimum
-                unsigned old = 0;
-                if (g.t == 0) old = atomicMin(best + item, nonce);
-                old = __shfl_sync(g.gmask, old, lane_off);
-                if (nonce < old) {
-                    if (g.t == 0 && old == 0xFFFFFFFFu) atomicAdd(&q->done_items, 1u);
-                    int got = 0;
-                    if (g.t == 0) {
-                        for (unsigned spin = 0; spin < kLockSpinLimit; ++spin) {
-                            if (atomicCAS(locks + item, 0u, 1u) == 0u) {
-                                got = 1;
-                                break;
-                            }
-                            __nanosleep(64);
-                        }
-                        if (!got) atomicOr(&q->error, 1u);
-                    }
-                    got = __shfl_sync(g.gmask, got, lane_off);
-                    if (got) {
-                        __threadfence();
-                        unsigned cur = 0;
-                        if (g.t == 0) cur = *reinterpret_cast<volatile unsigned *>(best + item);
-                        cur = __shfl_sync(g.gmask, cur, lane_off);
-                        if (cur == nonce) {
-                            const uint8_t *src = slot + C::SL_SIG;
-                            uint8_t *dst = sig_out + (size_t)item * sig_pitch;
-                            for (int b = g.t; b < PM::SIG_BYTES; b += 16) dst[b] = src[b];
-                        }
-                        __threadfence();
-                        __syncwarp(g.gmask);
-                        if (g.t == 0) atomicExch(locks + item, 0u);
-                    }
+                if (group_any(g, bad)) {
+                    rejected = true;
+                    break;
                 }
+            } else {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    x[m] = reduce32(x[m]);
+                    bad |= exceeds(x[m], PM::GAMMA2);
+                }
+                if (group_any(g, bad)) {
+                    rejected = true;
+                    break;
+                }
+                const uint8_t *w1p = slot + C::SL_W1P + (size_t)i * PM::POLYW1_PACKED;
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const int32_t w1 = (int32_t)get_bits(w1p, (g.t + 16 * m) * PM::W1_BITS, PM::W1_BITS);
+                    const unsigned h = make_hint<MODE>(r0[m] + x[m], w1);
+                    const unsigned bal = (__ballot_sync(g.gmask, h) >> lane_off) & 0xFFFFu;
+                    if (h) {
+                        const int idx = cnt + __popc(bal & ((1u << g.t) - 1u));
+                        if (idx < OMEGA) hs[idx] = (uint8_t)(g.t + 16 * m);
+                    }
+                    cnt += __popc(bal);
+                }
+                if (cnt > OMEGA) {
+                    rejected = true;
+                    break;
+                }
+                if (g.t == 0) hs[OMEGA + i] = (uint8_t)cnt;
             }
         }
+        if (g.t == 0) {
+            atomicAdd(&q->intt, (unsigned long long)n_intt);
+            atomicSub(arg.inflight + item, 1u);
+        }
+        if (rejected) return;
+        for (int qq = cnt + g.t; qq < OMEGA; qq += 16) hs[qq] = 0;
+        __syncwarp(g.gmask);
+        // accepted: lower the item's best nonce; publish if this attempt holds the minimum
+        unsigned old = 0;
+        if (g.t == 0) old = atomicMin(arg.best + item, nonce);
+        old = __shfl_sync(g.gmask, old, lane_off);
+        if (nonce >= old) return;
+        if (g.t == 0 && old == 0xFFFFFFFFu) {
+            atomicAdd(&q->done_items, 1u);
+            atomicSub(&s_ctl[CT_PEND], 1u);
+        }
+        int got = 0;
+        if (g.t == 0) {
+            for (unsigned spin = 0; spin < kLockSpinLimit; ++spin) {
+                if (atomicCAS(arg.locks + item, 0u, 1u) == 0u) {
+                    got = 1;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            if (!got) atomicOr(&q->error, 1u);
+        }
+        got = __shfl_sync(g.gmask, got, lane_off);
+        if (!got) return;
+        __threadfence();
+        unsigned cur = 0;
+        if (g.t == 0) cur = *reinterpret_cast<volatile unsigned *>(arg.best + item);
+        cur = __shfl_sync(g.gmask, cur, lane_off);
+        if (cur == nonce) {
+            const uint8_t *src = slot + C::SL_SIG;
+            uint8_t *dst = arg.sig_out + (size_t)item * arg.sig_pitch;
+            for (int b = g.t; b < PM::SIG_BYTES; b += 16) dst[b] = src[b];
+        }
+        __threadfence();
+        __syncwarp(g.gmask);
+        if (g.t == 0) atomicExch(arg.locks + item, 0u);
+    };
+
+    // w = invNTT(A_hat * NTT(y)), Decompose, pack w1 of one attempt (group-collective)
+    auto w_job = [&](int nb, int a) {
+        const unsigned item = s_item[nb * A + a];
+        uint8_t *slot = slot_of(nb, a);
+        const uint8_t *row = arg.cache + (size_t)arg.key_idx[item] * arg.cpitch;
+        int32_t *yh = reinterpret_cast<int32_t *>(ph) + (size_t)gi * (L * N + NTT_SMEM_WORDS);
+        g.sm = yh + L * N;
+#pragma unroll 1
+        for (int j = 0; j < L; ++j) {
+            int32_t x[16];
+            unpack_z_strided<MODE>(x, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
+            ntt16(x, g.sm, g.gmask, g.t);
+            store16_contig(yh + j * N + 16 * g.t, x);
+        }
+        __syncwarp(g.gmask);
+#pragma unroll 1
+        for (int i = 0; i < K; ++i) {
+            const int32_t *mat = reinterpret_cast<const int32_t *>(row + C::SK_MAT) + (size_t)i * L * N;
+            int32_t acc[16];
+#pragma unroll
+            for (int m = 0; m < 16; ++m) acc[m] = 0;
+#pragma unroll 1
+            for (int j = 0; j < L; ++j) {
+                int32_t av[16], yv[16];
+                load16_contig(av, mat + (size_t)j * N + 16 * g.t);
+                load16_contig(yv, yh + j * N + 16 * g.t);
+#pragma unroll
+                for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], yv[m]);
+            }
+#pragma unroll
+            for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m]);
+            intt16(acc, g.sm, g.gmask, g.t);
+            int32_t *w0 = reinterpret_cast<int32_t *>(slot + C::SL_W0) + (size_t)i * N;
+            int32_t w1[16];
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                int32_t a0;
+                w1[m] = decompose<MODE>(a0, caddq(acc[m]));
+                w0[g.t + 16 * m] = a0;
+            }
+            int32_t w1c[16];
+            strided_to_contig(g, w1, w1c);
+            uint32_t v[16];
+#pragma unroll
+            for (int m = 0; m < 16; ++m) v[m] = (uint32_t)w1c[m];
+            pack16_words<PM::W1_BITS>(
+                reinterpret_cast<uint32_t *>(slot + C::SL_W1P + (size_t)i * PM::POLYW1_PACKED + g.t * 2 * PM::W1_BITS), v);
+        }
+        __syncwarp(g.gmask);
+    };
+
+    // ---------------- NTT phase: rejection of batch cb (jobs < na_c), w = A y of batch nb
+    auto ntt_phase = [&](int cb, int na_c, int nb, int na_n) {
+        const int total = na_c + na_n;
+#pragma unroll 1
+        for (;;) {
+            int job = 0;
+            if (g.t == 0) job = (int)atomicAdd(&s_ctl[CT_NJOB], 1u);
+            job = __shfl_sync(g.gmask, job, lane_off);
+            if (job >= total) break;
+            if (job < na_c)
+                reject_job(cb, job);
+            else
+                w_job(nb, job - na_c);
+        }
+    };
+
+    // ---------------- main loop
+    if (tid == 0) s_ctl[CT_PEND] = n_own;
+    __syncthreads();
+    claim(0);
+    keccak_phase(0, 0, 0, (int)s_ctl[CT_NA0]);
+    __syncthreads();
+    ntt_phase(0, 0, 0, (int)s_ctl[CT_NA0]);
+    __syncthreads();
+    int cur = 0;
+#pragma unroll 1
+    for (;;) {
+        const int nxt = cur ^ 1;
+        claim(nxt);
+        const int na_c = (int)s_ctl[CT_NA0 + cur], na_n = (int)s_ctl[CT_NA0 + nxt];
+        // nothing in flight and nothing claimable: every owned item has its winner
+        if (na_c == 0 && na_n == 0) break;
+        keccak_phase(cur, na_c, nxt, na_n);
         __syncthreads();
+        ntt_phase(cur, na_c, nxt, na_n);
+        __syncthreads();
+        cur = nxt;
     }
 }
 
@@ -570,12 +622,12 @@ struct FusedVerifySmem {
     using PM = P<MODE>;
     static constexpr int G = THREADS / 16;
     static constexpr size_t PH_W = (size_t)G * ((PM::L + 1) * N * 4 + NTT_SMEM_WORDS * 4 + 32);
-    static constexpr size_t PH_C = (size_t)THREADS * (SHAKE256_RATE + 64);
+    static constexpr size_t PH_C = (size_t)THREADS * (34 + 16) * 4;
     static constexpr size_t BYTES = 256 + (PH_W > PH_C ? PH_W : PH_C);
 };
 
 template <int MODE, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_fused_verify(const uint8_t *cache, size_t cpitch, MsgRefs mr,
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const uint8_t *cache, size_t cpitch, MsgRefs mr,
                                                           const uint8_t *sig, size_t sig_pitch, int *ret,
                                                           uint8_t *scratch, FusedQueue *q) {
     using PM = P<MODE>;
@@ -626,12 +678,14 @@ __global__ void __launch_bounds__(THREADS) k_fused_verify(const uint8_t *cache, 
             uint2 ct[4];
 #pragma unroll
             for (int w = 0; w < 4; ++w) ct[w] = make_uint2(load_lane_bytes(s + 8 * w, 8).x, load_lane_bytes(s + 8 * w, 8).y);
-            uint8_t *blk = ph + (size_t)tid * SHAKE256_RATE;
-            uint32_t *mask = reinterpret_cast<uint32_t *>(ph + (size_t)THREADS * SHAKE256_RATE) + tid * 16;
-            sample_in_ball<PM::TAU>(ct, blk, mask);
+            uint32_t *blkw = reinterpret_cast<uint32_t *>(ph) + tid;
+            uint32_t *mask = reinterpret_cast<uint32_t *>(ph) + 34 * THREADS + tid;
+            sample_in_ball<PM::TAU, THREADS>(ct, blkw, mask);
             uint4 *mo = reinterpret_cast<uint4 *>(slot + C::VS_CM);
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) mo[kk] = make_uint4(mask[4 * kk], mask[4 * kk + 1], mask[4 * kk + 2], mask[4 * kk + 3]);
+            for (int kk = 0; kk < 4; ++kk)
+                mo[kk] = make_uint4(mask[(4 * kk) * THREADS], mask[(4 * kk + 1) * THREADS], mask[(4 * kk + 2) * THREADS],
+                                    mask[(4 * kk + 3) * THREADS]);
             reinterpret_cast<int *>(slot + C::VS_STATUS)[0] = status;
         }
         __syncthreads();
@@ -696,7 +750,7 @@ __global__ void __launch_bounds__(THREADS) k_fused_verify(const uint8_t *cache, 
                     int32_t acc[16];
 #pragma unroll
                     for (int m = 0; m < 16; ++m) acc[m] = 0;
-#pragma unroll
+#pragma unroll 1
                     for (int j = 0; j < L; ++j) {
                         int32_t av[16], zv[16];
                         load16_contig(av, mat + (size_t)j * N + 16 * g.t);

@@ -182,11 +182,12 @@ __global__ void __launch_bounds__(kBlock) k_sign_compute_w(const uint8_t *sign_p
     }
 }
 
-// SampleInBall(c~) (src/sign.cu:767-787), one thread per challenge.  The squeezed block and the
-// result live in this thread's slice of shared memory; the result is two 256-bit masks
-// (non-zero positions, negative positions).  blk: 136 bytes (8-aligned), mask: 16 words.
-template <int TAU>
-__device__ __forceinline__ void sample_in_ball(const uint2 (&ct)[4], uint8_t *blk, uint32_t *mask) {
+// SampleInBall(c~) (src/sign.cu:767-787), one thread per challenge.  The squeezed block (34
+// words) and the result (two 256-bit masks: non-zero positions, negative positions; 16 words) live
+// in shared memory interleaved across the threads of the block -- word k of this thread at
+// [k * STRIDE] -- so the dynamically indexed accesses of neighbouring threads hit distinct banks.
+template <int TAU, int STRIDE>
+__device__ __forceinline__ void sample_in_ball(const uint2 (&ct)[4], uint32_t *blkw, uint32_t *mask) {
     uint32_t al[25], ah[25];
     keccak_zero(al, ah);
 #pragma unroll
@@ -197,12 +198,14 @@ __device__ __forceinline__ void sample_in_ball(const uint2 (&ct)[4], uint8_t *bl
     al[4] = 0x1Fu;
     ah[16] ^= 0x80000000u;
     keccak_f1600(al, ah);
-    uint2 *b2 = reinterpret_cast<uint2 *>(blk);
 #pragma unroll
-    for (int w = 0; w < 17; ++w) b2[w] = make_uint2(al[w], ah[w]);
+    for (int w = 0; w < 17; ++w) {
+        blkw[(2 * w) * STRIDE] = al[w];
+        blkw[(2 * w + 1) * STRIDE] = ah[w];
+    }
     uint32_t sl = al[0], sh = ah[0];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) mask[k] = 0;
+    for (int k = 0; k < 16; ++k) mask[k * STRIDE] = 0;
     int pos = 8;
 #pragma unroll 1
     for (int i = N - TAU; i < N; ++i) {
@@ -211,20 +214,26 @@ __device__ __forceinline__ void sample_in_ball(const uint2 (&ct)[4], uint8_t *bl
             if (pos >= SHAKE256_RATE) {
                 keccak_f1600(al, ah);
 #pragma unroll
-                for (int w = 0; w < 17; ++w) b2[w] = make_uint2(al[w], ah[w]);
+                for (int w = 0; w < 17; ++w) {
+                    blkw[(2 * w) * STRIDE] = al[w];
+                    blkw[(2 * w + 1) * STRIDE] = ah[w];
+                }
                 pos = 0;
             }
-            b = blk[pos++];
+            b = (blkw[(pos >> 2) * STRIDE] >> (8 * (pos & 3))) & 0xFFu;
+            ++pos;
         } while (b > (uint32_t)i);
         const uint32_t wb = b >> 5, bb = 1u << (b & 31);
         const uint32_t wi = (uint32_t)i >> 5, bi = 1u << (i & 31);
-        const uint32_t ob = mask[wb] & bb, nb = mask[8 + wb] & bb;
+        uint32_t *occ_b = mask + wb * STRIDE, *neg_b = mask + (8 + wb) * STRIDE;
+        uint32_t *occ_i = mask + wi * STRIDE, *neg_i = mask + (8 + wi) * STRIDE;
+        const uint32_t ob = *occ_b & bb, nb = *neg_b & bb;
         // c[i] = c[b]
-        mask[wi] = ob ? (mask[wi] | bi) : (mask[wi] & ~bi);
-        mask[8 + wi] = nb ? (mask[8 + wi] | bi) : (mask[8 + wi] & ~bi);
+        *occ_i = ob ? (*occ_i | bi) : (*occ_i & ~bi);
+        *neg_i = nb ? (*neg_i | bi) : (*neg_i & ~bi);
         // c[b] = 1 - 2 * (signs & 1)
-        mask[wb] |= bb;
-        mask[8 + wb] = (sl & 1u) ? (mask[8 + wb] | bb) : (mask[8 + wb] & ~bb);
+        *occ_b |= bb;
+        *neg_b = (sl & 1u) ? (*neg_b | bb) : (*neg_b & ~bb);
         sl = (sl >> 1) | (sh << 31);
         sh >>= 1;
     }
@@ -235,8 +244,8 @@ __global__ void __launch_bounds__(kBlock) k_sign_challenge(const uint8_t *sign_p
                                                            const uint32_t *exec_lut, int nexec) {
     using PM = P<MODE>;
     using LY = Layout<MODE>;
-    __shared__ __align__(8) uint8_t s_blk[kBlock][SHAKE256_RATE];
-    __shared__ uint32_t s_mask[kBlock][16];
+    __shared__ uint32_t s_blk[2 * 17][kBlock];
+    __shared__ uint32_t s_mask[16][kBlock];
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nexec) return;
     const uint32_t item = exec_lut[e] >> 16;
@@ -251,11 +260,12 @@ __global__ void __launch_bounds__(kBlock) k_sign_challenge(const uint8_t *sign_p
     uint2 *sig_ct = reinterpret_cast<uint2 *>(trow + LY::TP_SIG);
 #pragma unroll
     for (int w = 0; w < 4; ++w) sig_ct[w] = ct[w];
-    uint32_t *mask = s_mask[threadIdx.x];
-    sample_in_ball<PM::TAU>(ct, s_blk[threadIdx.x], mask);
+    uint32_t *mask = &s_mask[0][threadIdx.x];
+    sample_in_ball<PM::TAU, kBlock>(ct, &s_blk[0][threadIdx.x], mask);
     uint4 *mo = reinterpret_cast<uint4 *>(trow + LY::TP_CMASK);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) mo[k] = make_uint4(mask[4 * k], mask[4 * k + 1], mask[4 * k + 2], mask[4 * k + 3]);
+    for (int k = 0; k < 4; ++k)
+        mo[k] = make_uint4(mask[(4 * k) * kBlock], mask[(4 * k + 1) * kBlock], mask[(4 * k + 2) * kBlock], mask[(4 * k + 3) * kBlock]);
 }
 
 // One group per attempt: c_hat = NTT(c); z = y + c*s1 (norm check, pack); r0 = w0 - c*s2 and c*t0

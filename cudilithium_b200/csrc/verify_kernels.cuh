@@ -17,8 +17,8 @@ __global__ void __launch_bounds__(kBlock) k_verify_prepare(uint8_t *pool, size_t
     using PM = P<MODE>;
     using LY = Layout<MODE>;
     constexpr int K = PM::K, OMEGA = PM::OMEGA;
-    __shared__ __align__(8) uint8_t s_blk[kBlock][SHAKE256_RATE];
-    __shared__ uint32_t s_mask[kBlock][16];
+    __shared__ uint32_t s_blk[2 * 17][kBlock];
+    __shared__ uint32_t s_mask[16][kBlock];
     const int it = blockIdx.x * blockDim.x + threadIdx.x;
     if (it >= n) return;
     uint8_t *row = pool + (size_t)it * pitch;
@@ -63,11 +63,12 @@ __global__ void __launch_bounds__(kBlock) k_verify_prepare(uint8_t *pool, size_t
 
     uint2 ct[4];
     ld_lanes(ct, row + LY::VF_SIG);
-    uint32_t *mask = s_mask[threadIdx.x];
-    sample_in_ball<PM::TAU>(ct, s_blk[threadIdx.x], mask);
+    uint32_t *mask = &s_mask[0][threadIdx.x];
+    sample_in_ball<PM::TAU, kBlock>(ct, &s_blk[0][threadIdx.x], mask);
     uint4 *mo = reinterpret_cast<uint4 *>(aux);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) mo[k] = make_uint4(mask[4 * k], mask[4 * k + 1], mask[4 * k + 2], mask[4 * k + 3]);
+    for (int k = 0; k < 4; ++k)
+        mo[k] = make_uint4(mask[(4 * k) * kBlock], mask[(4 * k + 1) * kBlock], mask[(4 * k + 2) * kBlock], mask[(4 * k + 3) * kBlock]);
     reinterpret_cast<int *>(aux + 64)[0] = status;
 }
 

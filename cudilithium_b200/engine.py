@@ -35,14 +35,20 @@ def pack_messages(msgs: list[bytes] | np.ndarray, device="cuda"):
 class Engine:
     """One cudil_engine (one parameter set, current device)."""
 
-    def __init__(self, mode: int, max_keys: int, max_items: int, threads: int = 0, budget_bytes: int = 0):
+    def __init__(self, mode: int, max_keys: int, max_items: int, threads: int = 0, budget_bytes: int = 0,
+                 spec_slots: int = 0):
+        """threads / spec_slots = 0 take the autotuned settings for this GPU (autotune.tuned)."""
+        from .autotune import tuned
         self.mode = mode
         self.params = _lib.params(mode)
         self.max_keys, self.max_items = max_keys, max_items
+        t = tuned(mode)
+        threads = threads or t["threads"]
         h = ctypes.c_void_p()
         check(lib.cudil_engine_create(ctypes.byref(h), mode, max_keys, max_items, threads, budget_bytes),
               "cudil_engine_create")
         self.h = h
+        self.set_spec_slots(spec_slots or t["spec_slots"])
 
     def close(self):
         if self.h:
@@ -58,6 +64,10 @@ class Engine:
     @property
     def device_bytes(self) -> int:
         return lib.cudil_engine_device_bytes(self.h)
+
+    def set_spec_slots(self, slots: int):
+        """Per-block target of signing attempts in flight; see cudil_engine_set_spec_slots."""
+        check(lib.cudil_engine_set_spec_slots(self.h, slots), "set_spec_slots")
 
     def info(self) -> dict:
         m, t, sb, vb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

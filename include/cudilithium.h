@@ -167,6 +167,12 @@ int cudil_engine_last_status(const cudil_engine *e, unsigned long long *attempts
 /* Work counters of the last completed signing batch: attempts run and inverse NTTs executed by the
  * rejection checks (for throughput accounting). */
 int cudil_engine_last_work(const cudil_engine *e, unsigned long long *attempts, unsigned long long *reject_intt);
+/* Signer tuning: per-block target of signing attempts in flight (1 .. 2 * threads_per_block).
+ * Every block owns a share of the batch's items; while it has many pending items each has at most
+ * two attempts in flight, and as they run out the remaining ones get up to target / pending
+ * consecutive nonces in flight (at most 64).  0 = default (threads_per_block).  Takes effect
+ * from the next batch. */
+int cudil_engine_set_spec_slots(cudil_engine *e, unsigned spec_slots);
 int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks);
 
 /* Peak of the 32-bit LOP3/funnel-shift mix Keccak-f[1600] issues: launches `blocks` x 256 threads
