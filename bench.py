@@ -385,7 +385,7 @@ def run_gpu(args) -> dict | None:
         "achieved": achieved, "peak": peak_ops / 1e9, "unit": "Gop/s",
         "frac": achieved / (peak_ops / 1e9) if achieved else None, "traffic": None,
         "ms_per_launch": g_ms, "launches": 1, "share_of_step": g_ms / total_ms if total_ms else None,
-        "attempts": att1, "reject_intt": intt1,
+        "attempts": att1, "reject_intt": intt1, "signer_phases": es.last_phases(),
         "ops_model": "Keccak-f1600 = 4560 LOP3/SHF ops; NTT 6144, invNTT 7168, Montgomery product 5",
         "peak_source": "measured live: k_alu_peak (3 LOP3 : 1 SHF at 64 ops/clk/SM; IMAD-heavy NTT work can "
                        "co-issue on the FMA pipe, so frac may exceed 1)",
@@ -696,7 +696,8 @@ def run_profile_case(args) -> dict:
         es.sign(sig, m, offs, lens, keys, stream=spp)
     torch.cuda.synchronize()
     es.last_status()
-    out = {"workload": args.workload, "batch": B, "engine": es.info(), "attempts": es.last_work()[0]}
+    out = {"workload": args.workload, "batch": B, "engine": es.info(), "attempts": es.last_work()[0],
+           "phases": es.last_phases()}
     if args.workload == "fused-verify":
         ev = Engine(mode, B, B, threads=args.engine_threads)
         ev.set_public_keys(pk, stream=spp)

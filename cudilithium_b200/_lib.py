@@ -93,6 +93,7 @@ SIGNATURES = {
                                     c_size_t, c_void_p]),
     "cudil_engine_last_status": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong), POINTER(c_uint32)]),
     "cudil_engine_last_work": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong), POINTER(ctypes.c_ulonglong)]),
+    "cudil_engine_last_phases": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong), POINTER(c_uint32)]),
     "cudil_engine_set_spec_slots": (c_int, [c_void_p, c_uint32]),
     "cudil_engine_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "cudil_alu_peak": (c_int, [c_void_p, c_int, c_int, c_void_p, POINTER(ctypes.c_double)]),

@@ -116,6 +116,13 @@ int cudil_engine_last_work(const cudil_engine *e, unsigned long long *attempts, 
     return CUDIL_OK;
 }
 
+int cudil_engine_last_phases(const cudil_engine *e, unsigned long long cycles[4], unsigned *iterations) {
+    if (!e || !e->impl) return CUDIL_ERR_INVALID;
+    for (int i = 0; i < 4; ++i) cycles[i] = e->impl->h_status->cyc[i];
+    if (iterations) *iterations = e->impl->h_status->iters;
+    return CUDIL_OK;
+}
+
 int cudil_engine_set_spec_slots(cudil_engine *e, unsigned spec_slots) { CUDIL_ENGINE_DISPATCH(e, set_spec_slots(spec_slots)); }
 
 int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks) {

@@ -66,8 +66,9 @@ struct FusedQueue {
     unsigned int n;            // items in the current batch
     unsigned int pad;
     unsigned long long intt;   // inverse NTTs run by the rejection checks (for work accounting)
-    unsigned int rr;           // round-robin probe position of the signer's work queue
+    unsigned int iters;        // signer block-iterations (summed over blocks)
     unsigned int pad2;
+    unsigned long long cyc[4]; // signer cycles per phase summed over blocks: claim, keccak, ntt, total
 };
 
 // ------------------------------------------------------------------ cache builders
@@ -227,7 +228,8 @@ static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *loc
         q->error = 0;
         q->attempts = 0;
         q->intt = 0;
-        q->rr = 0;
+        q->iters = 0;
+        for (int i = 0; i < 4; ++i) q->cyc[i] = 0;
     }
 }
 
@@ -236,9 +238,11 @@ static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *loc
 // Work queue.  Block b owns the items b, b + grid, b + 2*grid, ... and schedules them itself, so
 // refilling slots touches no shared counter.  Every owned item has a next-nonce counter and an
 // in-flight counter; a claim gives pending items (no accepted nonce yet) their next nonce, at most
-// D in flight per item.  D = 2 while the block has many pending items (one attempt being checked,
-// the next one already being computed) and grows up to 64 as its pending items run out, so the last
-// items of a block are speculated deeply instead of taking one rejection round after another.
+// D in flight per item, D = spec_slots / pending (1..64).  While a block owning many items has many
+// pending, D = 1 and each batch takes half of them, so the two batches in flight hold different
+// items and no attempt is wasted (blocks owning fewer than 64 items keep D >= 2 so both batches
+// stay fed); as pending items run out D grows up to 64, so the last items of a block are
+// speculated deeply instead of taking one rejection round after another.
 // Nonces of an item are issued in increasing order and every issued attempt completes before the
 // block exits, so the winner -- the smallest accepted nonce -- is the deterministic signature.
 //
@@ -297,20 +301,25 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
             const unsigned pend = s_ctl[CT_PEND];
             unsigned D = 0;
             if (pend) {
+                // depth 1 (alternating halves) needs enough owned items to fill both batches
+                const unsigned dmin = (n_own >= 64u) ? 1u : 2u;
                 const unsigned t = arg.spec_slots / pend;
-                D = t < 2u ? 2u : (t > 64u ? 64u : t);
+                D = t < dmin ? dmin : (t > 64u ? 64u : t);
             }
+            // With one attempt per item (D == 1) a batch takes at most half of the pending items, so
+            // the two batches in flight hold different items and no attempt is speculative.
+            const unsigned cap = (D == 1u) ? ((pend + 1u) / 2u < (unsigned)A ? (pend + 1u) / 2u : (unsigned)A) : (unsigned)A;
             unsigned filled = 0;
 #pragma unroll 1
-            for (unsigned pass = 0; pass < D && filled < (unsigned)A; ++pass) {
+            for (unsigned pass = 0; pass < D && filled < cap; ++pass) {
 #pragma unroll 1
-                for (unsigned k0 = 0; k0 < n_own && filled < (unsigned)A; k0 += 32) {
+                for (unsigned k0 = 0; k0 < n_own && filled < cap; k0 += 32) {
                     const unsigned k = k0 + lane, i = b0 + k * grid;
                     bool ok = false;
                     if (k < n_own && __ldcg(arg.best + i) == 0xFFFFFFFFu && __ldcg(arg.inflight + i) <= pass) ok = true;
                     const unsigned bal = __ballot_sync(0xFFFFFFFFu, ok);
                     const unsigned pos = filled + __popc(bal & ((1u << lane) - 1u));
-                    if (ok && pos < (unsigned)A) {
+                    if (ok && pos < cap) {
                         const unsigned nn = atomicAdd(arg.next_nonce + i, 1u);
                         if (nn < 65536u) {
                             atomicAdd(arg.inflight + i, 1u);
@@ -325,7 +334,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                         }
                     }
                     filled += __popc(bal);
-                    if (filled > (unsigned)A) filled = A;
+                    if (filled > cap) filled = cap;
                 }
             }
             if (lane == 0) {
@@ -343,10 +352,14 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         uint32_t *blkw = reinterpret_cast<uint32_t *>(ph) + tid;
         uint32_t *mask = reinterpret_cast<uint32_t *>(ph) + 34 * THREADS + tid;
         const int total = na_c + na_n * L;
+        // a warp takes 32 consecutive jobs at a time, so its lanes run the same job type together
 #pragma unroll 1
         for (;;) {
-            const int job = (int)atomicAdd(&s_ctl[CT_KJOB], 1u);
-            if (job >= total) break;
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(&s_ctl[CT_KJOB], 32u);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if ((int)base >= total) break;
+            const int job = (int)base + lane;
             if (job < na_c) {
                 const unsigned item = s_item[cb * A + job];
                 uint8_t *slot = slot_of(cb, job);
@@ -366,7 +379,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                 for (int k = 0; k < 4; ++k)
                     mo[k] = make_uint4(mask[(4 * k) * THREADS], mask[(4 * k + 1) * THREADS], mask[(4 * k + 2) * THREADS],
                                        mask[(4 * k + 3) * THREADS]);
-            } else {
+            } else if (job < total) {
                 const int idx = job - na_c, a = idx / L, j = idx % L;
                 const unsigned item = s_item[nb * A + a], nonce = s_nonce[nb * A + a];
                 uint2 rhop[8];
@@ -374,6 +387,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                 expand_mask_stream<MODE>(slot_of(nb, a) + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, rhop,
                                          (uint32_t)(L * nonce + j));
             }
+            __syncwarp();  // every lane runs the same grab / sync sequence
         }
     };
 
@@ -401,25 +415,31 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         }
         int32_t ch[16];
         challenge_strided(ch, masks, g.t);
-        ntt16(ch, g.sm, g.gmask, g.t);
+        ntt16_ool(ch, g.sm, g.gmask, g.t);
         const int32_t *s1 = reinterpret_cast<const int32_t *>(row + C::SK_S1);
         const int32_t *s2 = reinterpret_cast<const int32_t *>(row + C::SK_S2);
         const int32_t *t0 = reinterpret_cast<const int32_t *>(row + C::SK_T0);
         uint8_t *hs = slot + C::SL_SIG + PM::SIG_H;
         bool rejected = false;
         int cnt = 0, n_intt = 0;
-        int32_t r0[16];
-        // polynomial steps: z_0..z_{L-1}, then (r0_i, ct0_i) for i < K -- the order of the reference
+        int32_t r0[16], nx[16];
+        auto operand = [&](int step) -> const int32_t * {
+            if (step < L) return s1 + (size_t)step * N;
+            const int i = (step - L) >> 1;
+            return ((((step - L) & 1) == 0) ? s2 : t0) + (size_t)i * N;
+        };
+        load16_contig(nx, operand(0) + 16 * g.t);
+        // polynomial steps: z_0..z_{L-1}, then (r0_i, ct0_i) for i < K -- the order of the reference;
+        // the next step's operand is loaded while the current one transforms
 #pragma unroll 1
         for (int step = 0; step < L + 2 * K; ++step) {
             const int i = (step - L) >> 1;
             const bool is_z = step < L, is_r0 = !is_z && (((step - L) & 1) == 0);
-            const int32_t *src = is_z ? s1 + (size_t)step * N : (is_r0 ? s2 : t0) + (size_t)i * N;
             int32_t x[16];
-            load16_contig(x, src + 16 * g.t);
 #pragma unroll
-            for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
-            intt16(x, g.sm, g.gmask, g.t);
+            for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], nx[m]);
+            if (step + 1 < L + 2 * K) load16_contig(nx, operand(step + 1) + 16 * g.t);
+            intt16_ool(x, g.sm, g.gmask, g.t);
             ++n_intt;
             bool bad = false;
             if (is_z) {
@@ -515,9 +535,26 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         if (g.t == 0) cur = *reinterpret_cast<volatile unsigned *>(arg.best + item);
         cur = __shfl_sync(g.gmask, cur, lane_off);
         if (cur == nonce) {
-            const uint8_t *src = slot + C::SL_SIG;
+            // the staged signature is 256-byte aligned; the output row may only be byte aligned
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(slot + C::SL_SIG);
             uint8_t *dst = arg.sig_out + (size_t)item * arg.sig_pitch;
-            for (int b = g.t; b < PM::SIG_BYTES; b += 16) dst[b] = src[b];
+            constexpr int NW = (PM::SIG_BYTES + 3) / 4;
+#pragma unroll 1
+            for (int w0 = 0; w0 < NW; w0 += 16 * 8) {
+                uint32_t w[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int wi = w0 + g.t + 16 * k;
+                    w[k] = (wi < NW) ? src[wi] : 0u;
+                }
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int wi = w0 + g.t + 16 * k;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        if (wi < NW && 4 * wi + b < PM::SIG_BYTES) dst[4 * wi + b] = (uint8_t)(w[k] >> (8 * b));
+                }
+            }
         }
         __threadfence();
         __syncwarp(g.gmask);
@@ -535,27 +572,37 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         for (int j = 0; j < L; ++j) {
             int32_t x[16];
             unpack_z_strided<MODE>(x, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
-            ntt16(x, g.sm, g.gmask, g.t);
-            store16_contig(yh + j * N + 16 * g.t, x);
+            ntt16_ool(x, g.sm, g.gmask, g.t);
+            store16_smem(yh + j * N, x, g.t);
         }
         __syncwarp(g.gmask);
+        const int32_t *mat0 = reinterpret_cast<const int32_t *>(row + C::SK_MAT);
 #pragma unroll 1
         for (int i = 0; i < K; ++i) {
-            const int32_t *mat = reinterpret_cast<const int32_t *>(row + C::SK_MAT) + (size_t)i * L * N;
             int32_t acc[16];
 #pragma unroll
             for (int m = 0; m < 16; ++m) acc[m] = 0;
+            // A row entries in chunks of up to four polynomials: their loads are all in flight
+            // before the first one is consumed
 #pragma unroll 1
-            for (int j = 0; j < L; ++j) {
-                int32_t av[16], yv[16];
-                load16_contig(av, mat + (size_t)j * N + 16 * g.t);
-                load16_contig(yv, yh + j * N + 16 * g.t);
+            for (int j0 = 0; j0 < L; j0 += 4) {
+                int32_t av[4][16];
 #pragma unroll
-                for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], yv[m]);
+                for (int jj = 0; jj < 4; ++jj)
+                    if (j0 + jj < L) load16_contig(av[jj], mat0 + ((size_t)i * L + j0 + jj) * N + 16 * g.t);
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) {
+                    if (j0 + jj < L) {
+                        int32_t yv[16];
+                        load16_smem(yv, yh + (j0 + jj) * N, g.t);
+#pragma unroll
+                        for (int m = 0; m < 16; ++m) acc[m] += montmul(av[jj][m], yv[m]);
+                    }
+                }
             }
 #pragma unroll
             for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m]);
-            intt16(acc, g.sm, g.gmask, g.t);
+            intt16_ool(acc, g.sm, g.gmask, g.t);
             int32_t *w0 = reinterpret_cast<int32_t *>(slot + C::SL_W0) + (size_t)i * N;
             int32_t w1[16];
 #pragma unroll
@@ -578,20 +625,28 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
     // ---------------- NTT phase: rejection of batch cb (jobs < na_c), w = A y of batch nb
     auto ntt_phase = [&](int cb, int na_c, int nb, int na_n) {
         const int total = na_c + na_n;
+        // a warp takes two consecutive jobs, one per 16-thread group, so both groups of the warp
+        // usually run the same job type in lockstep
 #pragma unroll 1
         for (;;) {
-            int job = 0;
-            if (g.t == 0) job = (int)atomicAdd(&s_ctl[CT_NJOB], 1u);
-            job = __shfl_sync(g.gmask, job, lane_off);
-            if (job >= total) break;
-            if (job < na_c)
-                reject_job(cb, job);
-            else
-                w_job(nb, job - na_c);
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(&s_ctl[CT_NJOB], 2u);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if ((int)base >= total) break;
+            const int job = (int)base + (lane_off ? 1 : 0);
+            if (job < total) {
+                if (job < na_c)
+                    reject_job(cb, job);
+                else
+                    w_job(nb, job - na_c);
+            }
+            __syncwarp();  // both groups back together before the next full-warp grab
         }
     };
 
-    // ---------------- main loop
+    // ---------------- main loop (thread 0 accumulates per-phase cycles for the work counters)
+    long long t_claim = 0, t_kec = 0, t_ntt = 0, t_start = clock64(), t0;
+    unsigned iters = 0;
     if (tid == 0) s_ctl[CT_PEND] = n_own;
     __syncthreads();
     claim(0);
@@ -603,15 +658,29 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
 #pragma unroll 1
     for (;;) {
         const int nxt = cur ^ 1;
+        t0 = clock64();
         claim(nxt);
+        t_claim += clock64() - t0;
         const int na_c = (int)s_ctl[CT_NA0 + cur], na_n = (int)s_ctl[CT_NA0 + nxt];
         // nothing in flight and nothing claimable: every owned item has its winner
         if (na_c == 0 && na_n == 0) break;
+        ++iters;
+        t0 = clock64();
         keccak_phase(cur, na_c, nxt, na_n);
         __syncthreads();
+        t_kec += clock64() - t0;
+        t0 = clock64();
         ntt_phase(cur, na_c, nxt, na_n);
         __syncthreads();
+        t_ntt += clock64() - t0;
         cur = nxt;
+    }
+    if (tid == 0) {
+        atomicAdd(&q->cyc[0], (unsigned long long)t_claim);
+        atomicAdd(&q->cyc[1], (unsigned long long)t_kec);
+        atomicAdd(&q->cyc[2], (unsigned long long)t_ntt);
+        atomicAdd(&q->cyc[3], (unsigned long long)(clock64() - t_start));
+        atomicAdd(&q->iters, iters);
     }
 }
 
@@ -639,12 +708,15 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
     const int tid = threadIdx.x, gi = tid >> 4, lane = tid & 31;
     const unsigned n = q->n;
     uint8_t *my_slots = scratch + (size_t)blockIdx.x * A * C::VSLOT;
+    // chunks of at most A signatures, small enough that every block of the grid gets work
+    unsigned chunk = (n + gridDim.x - 1) / gridDim.x;
+    chunk = chunk < 1u ? 1u : (chunk > (unsigned)A ? (unsigned)A : chunk);
     for (;;) {
-        if (tid == 0) s_ctl[0] = (unsigned)atomicAdd(&q->next_ticket, (unsigned long long)A);
+        if (tid == 0) s_ctl[0] = (unsigned)atomicAdd(&q->next_ticket, (unsigned long long)chunk);
         __syncthreads();
         const unsigned base = s_ctl[0];
         if (base >= n) break;
-        const int na = (int)((n - base) < (unsigned)A ? (n - base) : (unsigned)A);
+        const int na = (int)((n - base) < chunk ? (n - base) : chunk);
 
         // hint encoding checks, mu = H(tr||m), c = SampleInBall(c~): thread per signature
         if (tid < na) {
@@ -716,7 +788,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
                         zbad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
                     }
                     ntt16(x, g.sm, g.gmask, g.t);
-                    store16_contig(zh + j * N + 16 * g.t, x);
+                    store16_smem(zh + j * N, x, g.t);
                 }
                 if (group_any(g, zbad) && g.t == 0) reinterpret_cast<int *>(slot + C::VS_STATUS)[0] |= 2;
                 {
@@ -733,7 +805,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
                     int32_t x[16];
                     challenge_strided(x, masks, g.t);
                     ntt16(x, g.sm, g.gmask, g.t);
-                    store16_contig(zh + L * N + 16 * g.t, x);
+                    store16_smem(zh + L * N, x, g.t);
                 }
                 __syncwarp(g.gmask);
                 const uint8_t *h = s + PM::SIG_H;
@@ -754,12 +826,12 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
                     for (int j = 0; j < L; ++j) {
                         int32_t av[16], zv[16];
                         load16_contig(av, mat + (size_t)j * N + 16 * g.t);
-                        load16_contig(zv, zh + j * N + 16 * g.t);
+                        load16_smem(zv, zh + j * N, g.t);
 #pragma unroll
                         for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], zv[m]);
                     }
                     int32_t cv[16], tv[16];
-                    load16_contig(cv, zh + L * N + 16 * g.t);
+                    load16_smem(cv, zh + L * N, g.t);
                     load16_contig(tv, reinterpret_cast<const int32_t *>(row + C::PK_T1) + (size_t)i * N + 16 * g.t);
 #pragma unroll
                     for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m] - montmul(cv[m], tv[m]));

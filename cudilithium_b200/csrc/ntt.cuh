@@ -168,6 +168,41 @@ __device__ __forceinline__ void intt16(int32_t (&x)[16], int32_t *sm, unsigned g
     for (int i = 0; i < 16; ++i) x[i] = montmul_pre(x[i], F_INV, F_INV_Q);
 }
 
+// Out-of-line forms of the two transforms for large kernels that call them from many places: one
+// copy of each transform instead of one per call site keeps the instruction working set small.
+// The 16 coefficients travel by value (registers), not through memory.
+struct Coef16 {
+    int32_t v[16];
+};
+
+static __device__ __noinline__ Coef16 ntt16_call(Coef16 x, int32_t *sm, unsigned gmask, int t) {
+    ntt16(x.v, sm, gmask, t);
+    return x;
+}
+
+static __device__ __noinline__ Coef16 intt16_call(Coef16 x, int32_t *sm, unsigned gmask, int t) {
+    intt16(x.v, sm, gmask, t);
+    return x;
+}
+
+__device__ __forceinline__ void ntt16_ool(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
+    Coef16 c;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) c.v[i] = x[i];
+    c = ntt16_call(c, sm, gmask, t);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = c.v[i];
+}
+
+__device__ __forceinline__ void intt16_ool(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
+    Coef16 c;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) c.v[i] = x[i];
+    c = intt16_call(c, sm, gmask, t);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = c.v[i];
+}
+
 // 64 contiguous bytes (natural-order NTT-domain slice 16t..16t+15) <-> registers.
 __device__ __forceinline__ void load16_contig(int32_t (&x)[16], const int32_t *p) {
     const int4 *q = reinterpret_cast<const int4 *>(p);
@@ -185,6 +220,26 @@ __device__ __forceinline__ void store16_contig(int32_t *p, const int32_t (&x)[16
     int4 *q = reinterpret_cast<int4 *>(p);
 #pragma unroll
     for (int i = 0; i < 4; ++i) q[i] = make_int4(x[4 * i], x[4 * i + 1], x[4 * i + 2], x[4 * i + 3]);
+}
+
+// The same 64-byte slice in shared memory with its four 16-byte chunks rotated by t, so the
+// 128-bit accesses of neighbouring threads (64 bytes apart) fall into different banks.
+__device__ __forceinline__ void store16_smem(int32_t *poly, const int32_t (&x)[16], int t) {
+    int4 *q = reinterpret_cast<int4 *>(poly + 16 * t);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[(i + t) & 3] = make_int4(x[4 * i], x[4 * i + 1], x[4 * i + 2], x[4 * i + 3]);
+}
+
+__device__ __forceinline__ void load16_smem(int32_t (&x)[16], const int32_t *poly, int t) {
+    const int4 *q = reinterpret_cast<const int4 *>(poly + 16 * t);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int4 v = q[(i + t) & 3];
+        x[4 * i] = v.x;
+        x[4 * i + 1] = v.y;
+        x[4 * i + 2] = v.z;
+        x[4 * i + 3] = v.w;
+    }
 }
 
 // Strided slice a[t + 16 i] <-> registers (coalesced across the group).

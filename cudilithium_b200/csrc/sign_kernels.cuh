@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_compute_w(const uint8_t *sign_p
         int32_t x[16];
         unpack_z_strided<MODE>(x, temp_pool + (size_t)e * tp + LY::TP_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
         ntt16(x, g.sm, g.gmask, g.t);
-        store16_contig(&s_yhat[a][j][16 * g.t], x);
+        store16_smem(&s_yhat[a][j][0], x, g.t);
     }
     __syncthreads();
     for (int u = gi; u < AW * K; u += kGroupsPerBlock) {
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_compute_w(const uint8_t *sign_p
         for (int j = 0; j < L; ++j) {
             int32_t av[16], yv[16];
             load16_contig(av, mat + (size_t)j * N + 16 * g.t);
-            load16_contig(yv, &s_yhat[a][j][16 * g.t]);
+            load16_smem(yv, &s_yhat[a][j][0], g.t);
 #pragma unroll
             for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], yv[m]);
         }
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_challenge(const uint8_t *sign_p
 // (norm checks); MakeHint (at most OMEGA, positions in ascending order).  On acceptance the temp
 // row holds the complete signature and done[e] = 1 (src/sign.cu:1010-1195).
 template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_sign_reject(const uint8_t *sign_pool, size_t sp, size_t mlen, uint8_t *temp_pool,
+__global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_pool, size_t sp, size_t mlen, uint8_t *temp_pool,
                                                         size_t tp, const uint32_t *exec_lut, uint8_t *done, int nexec) {
     using PM = P<MODE>;
     using LY = Layout<MODE>;
@@ -301,74 +301,77 @@ __global__ void __launch_bounds__(kBlock) k_sign_reject(const uint8_t *sign_pool
     challenge_strided(ch, masks, g.t);
     ntt16(ch, g.sm, g.gmask, g.t);
 
-    // z = y + invNTT(c_hat * s1_hat), ||z|| < gamma1 - beta
+    // polynomial steps in the reference's order: z_0..z_{L-1}, then (r0_i, ct0_i) for i < K; one
+    // inverse-NTT call site, the next step's operand is loaded while the current one transforms
     const int32_t *s1 = reinterpret_cast<const int32_t *>(srow + LY::sg_s1(mlen));
-    for (int j = 0; j < L; ++j) {
-        int32_t x[16], y[16];
-        load16_contig(x, s1 + (size_t)j * N + 16 * g.t);
-#pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
-        intt16(x, g.sm, g.gmask, g.t);
-        unpack_z_strided<MODE>(y, trow + LY::TP_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
-        bool bad = false;
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            x[m] = reduce32(x[m] + y[m]);
-            bad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
-        }
-        if (group_any(g, bad)) return;
-        int32_t zc[16];
-        strided_to_contig(g, x, zc);
-        uint32_t v[16];
-#pragma unroll
-        for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
-        pack16_words<PM::Z_BITS>(
-            reinterpret_cast<uint32_t *>(trow + LY::TP_SIG + PM::SIG_Z + (size_t)j * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
-    }
-
     const int32_t *s2 = reinterpret_cast<const int32_t *>(srow + LY::sg_s2(mlen));
     const int32_t *t0 = reinterpret_cast<const int32_t *>(srow + LY::sg_t0(mlen));
+    auto operand = [&](int step) -> const int32_t * {
+        if (step < L) return s1 + (size_t)step * N;
+        const int i = (step - L) >> 1;
+        return ((((step - L) & 1) == 0) ? s2 : t0) + (size_t)i * N;
+    };
     uint8_t *hs = trow + LY::TP_SIG + PM::SIG_H;
+    const int lane_off = threadIdx.x & 16;
     int cnt = 0;
-    for (int i = 0; i < K; ++i) {
-        int32_t x[16], r0[16];
-        load16_contig(x, s2 + (size_t)i * N + 16 * g.t);
+    int32_t r0[16], nx[16];
+    load16_contig(nx, operand(0) + 16 * g.t);
+#pragma unroll 1
+    for (int step = 0; step < L + 2 * K; ++step) {
+        const int i = (step - L) >> 1;
+        const bool is_z = step < L, is_r0 = !is_z && (((step - L) & 1) == 0);
+        int32_t x[16];
 #pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
+        for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], nx[m]);
+        if (step + 1 < L + 2 * K) load16_contig(nx, operand(step + 1) + 16 * g.t);
         intt16(x, g.sm, g.gmask, g.t);
-        const int32_t *w0 = reinterpret_cast<const int32_t *>(trow + LY::TP_W0) + (size_t)i * N;
         bool bad = false;
+        if (is_z) {
+            int32_t y[16];
+            unpack_z_strided<MODE>(y, trow + LY::TP_Y + (size_t)step * PM::POLYZ_PACKED, g.t);
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            r0[m] = reduce32(w0[g.t + 16 * m] - x[m]);
-            bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
-        }
-        if (group_any(g, bad)) return;
-        load16_contig(x, t0 + (size_t)i * N + 16 * g.t);
-#pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], x[m]);
-        intt16(x, g.sm, g.gmask, g.t);
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            x[m] = reduce32(x[m]);
-            bad |= exceeds(x[m], PM::GAMMA2);
-        }
-        if (group_any(g, bad)) return;
-        const uint8_t *w1p = trow + LY::TP_W1P + (size_t)i * PM::POLYW1_PACKED;
-        const int lane_off = threadIdx.x & 16;
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const int32_t w1 = (int32_t)get_bits(w1p, (g.t + 16 * m) * PM::W1_BITS, PM::W1_BITS);
-            const unsigned h = make_hint<MODE>(r0[m] + x[m], w1);
-            const unsigned bal = (__ballot_sync(g.gmask, h) >> lane_off) & 0xFFFFu;
-            if (h) {
-                const int idx = cnt + __popc(bal & ((1u << g.t) - 1u));
-                if (idx < OMEGA) hs[idx] = (uint8_t)(g.t + 16 * m);
+            for (int m = 0; m < 16; ++m) {
+                x[m] = reduce32(x[m] + y[m]);
+                bad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
             }
-            cnt += __popc(bal);
+            if (group_any(g, bad)) return;
+            int32_t zc[16];
+            strided_to_contig(g, x, zc);
+            uint32_t v[16];
+#pragma unroll
+            for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
+            pack16_words<PM::Z_BITS>(
+                reinterpret_cast<uint32_t *>(trow + LY::TP_SIG + PM::SIG_Z + (size_t)step * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
+        } else if (is_r0) {
+            const int32_t *w0 = reinterpret_cast<const int32_t *>(trow + LY::TP_W0) + (size_t)i * N;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                r0[m] = reduce32(w0[g.t + 16 * m] - x[m]);
+                bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
+            }
+            if (group_any(g, bad)) return;
+        } else {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                x[m] = reduce32(x[m]);
+                bad |= exceeds(x[m], PM::GAMMA2);
+            }
+            if (group_any(g, bad)) return;
+            const uint8_t *w1p = trow + LY::TP_W1P + (size_t)i * PM::POLYW1_PACKED;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                const int32_t w1 = (int32_t)get_bits(w1p, (g.t + 16 * m) * PM::W1_BITS, PM::W1_BITS);
+                const unsigned h = make_hint<MODE>(r0[m] + x[m], w1);
+                const unsigned bal = (__ballot_sync(g.gmask, h) >> lane_off) & 0xFFFFu;
+                if (h) {
+                    const int idx = cnt + __popc(bal & ((1u << g.t) - 1u));
+                    if (idx < OMEGA) hs[idx] = (uint8_t)(g.t + 16 * m);
+                }
+                cnt += __popc(bal);
+            }
+            if (cnt > OMEGA) return;
+            if (g.t == 0) hs[OMEGA + i] = (uint8_t)cnt;
         }
-        if (cnt > OMEGA) return;
-        if (g.t == 0) hs[OMEGA + i] = (uint8_t)cnt;
     }
     for (int q = cnt + g.t; q < OMEGA; q += 16) hs[q] = 0;
     if (g.t == 0) done[e] = 1;

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kBlock) k_verify_w(uint8_t *pool, size_t pitch
             challenge_strided(x, masks, g.t);
         }
         ntt16(x, g.sm, g.gmask, g.t);
-        store16_contig(&s_hat[a][j][16 * g.t], x);
+        store16_smem(&s_hat[a][j][0], x, g.t);
     }
     __syncthreads();
 
@@ -147,12 +147,12 @@ __global__ void __launch_bounds__(kBlock) k_verify_w(uint8_t *pool, size_t pitch
         for (int j = 0; j < L; ++j) {
             int32_t av[16], zv[16];
             load16_contig(av, mat + (size_t)j * N + 16 * g.t);
-            load16_contig(zv, &s_hat[a][j][16 * g.t]);
+            load16_smem(zv, &s_hat[a][j][0], g.t);
 #pragma unroll
             for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], zv[m]);
         }
         int32_t cv[16];
-        load16_contig(cv, &s_hat[a][L][16 * g.t]);
+        load16_smem(cv, &s_hat[a][L][0], g.t);
 #pragma unroll
         for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m] - montmul(cv[m], t1[m]));
         intt16(acc, g.sm, g.gmask, g.t);

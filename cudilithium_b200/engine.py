@@ -112,6 +112,13 @@ class Engine:
         lib.cudil_engine_last_work(self.h, ctypes.byref(a), ctypes.byref(i))
         return a.value, i.value
 
+    def last_phases(self) -> dict:
+        """Signer phase profile of the last batch (block-summed SM cycles and iterations)."""
+        cyc = (ctypes.c_ulonglong * 4)()
+        it = ctypes.c_uint32()
+        lib.cudil_engine_last_phases(self.h, cyc, ctypes.byref(it))
+        return {"claim": cyc[0], "keccak": cyc[1], "ntt": cyc[2], "total": cyc[3], "iterations": it.value}
+
     # ---- numpy conveniences (synchronous)
     def sign_np(self, msgs, key_idx) -> np.ndarray:
         d_msgs, offs, lens = pack_messages(msgs)

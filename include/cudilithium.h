@@ -173,6 +173,9 @@ int cudil_engine_last_work(const cudil_engine *e, unsigned long long *attempts, 
  * consecutive nonces in flight (at most 64).  0 = default (threads_per_block).  Takes effect
  * from the next batch. */
 int cudil_engine_set_spec_slots(cudil_engine *e, unsigned spec_slots);
+/* Signer phase profile of the last batch: SM cycles summed over blocks spent in slot refills,
+ * Keccak phases, NTT phases and in total, and the number of block iterations. */
+int cudil_engine_last_phases(const cudil_engine *e, unsigned long long cycles[4], unsigned *iterations);
 int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks);
 
 /* Peak of the 32-bit LOP3/funnel-shift mix Keccak-f[1600] issues: launches `blocks` x 256 threads
