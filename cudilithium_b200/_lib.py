@@ -58,6 +58,17 @@ class cudil_task_lut(ctypes.Structure):
     ]
 
 
+class cudil_serve_config(ctypes.Structure):
+    _fields_ = [("device_budget_bytes", c_size_t), ("path", c_int32), ("slots_per_lane", c_int32),
+                ("max_batch", c_int32), ("engine_threads", c_int32), ("engine_spec_slots", c_int32),
+                ("plain_exec_threshold", c_int32), ("max_mlen", c_uint32), ("reserved", c_uint32)]
+
+
+class cudil_serve_stats(ctypes.Structure):
+    _fields_ = [("wall_s", ctypes.c_double), ("batches", c_size_t), ("slots", c_size_t),
+                ("device_bytes", c_size_t)]
+
+
 # Every symbol the public header declares, with its ctypes signature.
 SIGNATURES = {
     "cudil_version": (c_char_p, []),
@@ -79,6 +90,11 @@ SIGNATURES = {
     "cudil_verify_dev": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
                                  c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
     "cudil_ntt_mul": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "cudil_sign_dev_varlen": (c_int, [c_int, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p,
+                                      c_void_p, c_size_t, c_void_p, c_size_t, POINTER(cudil_task_lut), c_size_t,
+                                      c_size_t, c_void_p]),
+    "cudil_verify_dev_varlen": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_void_p,
+                                        c_size_t, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
     "cudil_verify_noalloc_max_batch": (c_size_t, [c_int, c_size_t]),
     "cudil_verify_noalloc": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
                                      c_void_p, c_size_t, c_void_p]),
@@ -86,6 +102,7 @@ SIGNATURES = {
     "cudil_engine_destroy": (c_int, [c_void_p]),
     "cudil_engine_device_bytes": (c_size_t, [c_void_p]),
     "cudil_engine_set_secret_keys": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
+    "cudil_engine_attach_keys": (c_int, [c_void_p, c_void_p]),
     "cudil_engine_set_public_keys": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
     "cudil_engine_sign": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_size_t,
                                   c_void_p]),
@@ -96,6 +113,9 @@ SIGNATURES = {
     "cudil_engine_last_phases": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong), POINTER(c_uint32)]),
     "cudil_engine_set_spec_slots": (c_int, [c_void_p, c_uint32]),
     "cudil_engine_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    "cudil_serve_trace": (c_int, [POINTER(cudil_serve_config), POINTER(c_void_p), POINTER(c_void_p),
+                                  POINTER(c_size_t), c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_size_t,
+                                  c_void_p, POINTER(cudil_serve_stats)]),
     "cudil_alu_peak": (c_int, [c_void_p, c_int, c_int, c_void_p, POINTER(ctypes.c_double)]),
     "cudil_launch_count": (ctypes.c_ulonglong, []),
     "cudil_kernel_timing": (None, [c_int]),

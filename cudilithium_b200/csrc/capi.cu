@@ -178,6 +178,25 @@ int cudil_verify_dev(int mode, int *d_ret, const uint8_t *d_sig, size_t sig_pitc
                                    pitch, batch, (cudaStream_t)stream, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice))
 }
 
+int cudil_sign_dev_varlen(int mode, uint8_t *d_sig, size_t sig_pitch, const uint8_t *d_m, size_t m_pitch,
+                          const uint32_t *d_mlens, size_t max_mlen, const uint8_t *d_sk, uint8_t *d_sign_pool,
+                          size_t sign_pitch, uint8_t *d_temp_pool, size_t temp_pitch, cudil_task_lut *lut,
+                          size_t exec_threshold, size_t batch, void *stream) {
+    if (!d_mlens) return CUDIL_ERR_INVALID;
+    CUDIL_DISPATCH(mode, I::sign(d_sig, sig_pitch, nullptr, d_m, m_pitch, max_mlen, d_sk, I::PM::SK_BYTES, d_sign_pool,
+                                 sign_pitch, d_temp_pool, temp_pitch, lut, exec_threshold, batch, (cudaStream_t)stream,
+                                 cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice, d_mlens))
+}
+
+int cudil_verify_dev_varlen(int mode, int *d_ret, const uint8_t *d_sig, size_t sig_pitch, size_t siglen,
+                            const uint8_t *d_m, size_t m_pitch, const uint32_t *d_mlens, size_t max_mlen,
+                            const uint8_t *d_pk, uint8_t *d_pool, size_t pitch, size_t batch, void *stream) {
+    if (!d_mlens) return CUDIL_ERR_INVALID;
+    CUDIL_DISPATCH(mode, I::verify(d_ret, d_sig, sig_pitch, siglen, d_m, m_pitch, max_mlen, d_pk, I::PM::PK_BYTES, d_pool,
+                                   pitch, batch, (cudaStream_t)stream, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice,
+                                   d_mlens))
+}
+
 int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t npolys, void *stream) {
     if (npolys == 0) return CUDIL_OK;
     if (!d_a || !d_b || !d_out) return CUDIL_ERR_INVALID;

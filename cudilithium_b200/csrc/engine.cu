@@ -123,6 +123,11 @@ int cudil_engine_last_phases(const cudil_engine *e, unsigned long long cycles[4]
     return CUDIL_OK;
 }
 
+int cudil_engine_attach_keys(cudil_engine *e, const cudil_engine *src) {
+    if (!src || !src->impl) return CUDIL_ERR_INVALID;
+    CUDIL_ENGINE_DISPATCH(e, attach_keys(src->impl));
+}
+
 int cudil_engine_set_spec_slots(cudil_engine *e, unsigned spec_slots) { CUDIL_ENGINE_DISPATCH(e, set_spec_slots(spec_slots)); }
 
 int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks) {

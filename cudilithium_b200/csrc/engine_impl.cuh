@@ -43,6 +43,7 @@ struct EngineBase {
     const void *g_sign_key[2] = {nullptr, nullptr}, *g_verify_key[2] = {nullptr, nullptr};
     cudaStream_t g_sign_stream = nullptr, g_verify_stream = nullptr;
     size_t device_bytes = 0;
+    bool owns_cache = true;  // false when the key caches belong to another engine (attach_keys)
     virtual ~EngineBase() = default;
 };
 
@@ -65,8 +66,11 @@ struct EngineImpl : EngineBase {
     // Device bytes the engine needs (the admission budget checks this before allocating).
     static size_t required_bytes(size_t max_keys, size_t max_items, int threads, int sign_grid, int verify_grid) {
         return max_keys * (align256(C::SK_ROW) + align256(C::PK_ROW)) + max_items * (C::ITEM_BYTES + 4 * sizeof(unsigned)) +
-               stage_bytes(max_items) + sizeof(FusedQueue) +
-               std::max((size_t)sign_grid * 2 * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
+               stage_bytes(max_items) + sizeof(FusedQueue) + scratch_for(max_items, threads, sign_grid, verify_grid);
+    }
+    static size_t scratch_for(size_t max_items, int threads, int sign_grid, int verify_grid) {
+        if (max_items == 0) return 0;
+        return std::max((size_t)sign_grid * 2 * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
     }
 
     template <int T>
@@ -86,7 +90,8 @@ struct EngineImpl : EngineBase {
         max_keys = mk;
         max_items = mi;
         threads = thr;
-        if (mk == 0 || mi == 0 || mi > (1u << 24)) return CUDIL_ERR_INVALID;
+        // mk == 0: caches attached later; mi == 0: a cache-only engine other engines attach to
+        if ((mi == 0 && mk == 0) || mi > (1u << 24)) return CUDIL_ERR_INVALID;
         if (cudaGetDevice(&device) != cudaSuccess) return CUDIL_ERR_CUDA;
         if (cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return CUDIL_ERR_CUDA;
         int rc = (threads == 128) ? configure<128>() : (threads == 256 ? configure<256>() : CUDIL_ERR_INVALID);
@@ -96,17 +101,20 @@ struct EngineImpl : EngineBase {
         if (budget && device_bytes > budget) return CUDIL_ERR_BUDGET;
         sk_pitch = align256(C::SK_ROW);
         pk_pitch = align256(C::PK_ROW);
-        scratch_bytes = std::max((size_t)sign_grid * 2 * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
+        scratch_bytes = scratch_for(mi, threads, sign_grid, verify_grid);
         spec_slots = (unsigned)threads;
-        if (cudaMalloc(&sk_cache, mk * sk_pitch) != cudaSuccess || cudaMalloc(&pk_cache, mk * pk_pitch) != cudaSuccess ||
-            cudaMalloc(&items, mi * C::ITEM_BYTES) != cudaSuccess || cudaMalloc(&best, mi * sizeof(unsigned)) != cudaSuccess ||
-            cudaMalloc(&locks, mi * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&q, sizeof(FusedQueue)) != cudaSuccess ||
-            cudaMalloc(&next_nonce, mi * sizeof(unsigned)) != cudaSuccess ||
-            cudaMalloc(&inflight, mi * sizeof(unsigned)) != cudaSuccess ||
-            cudaMalloc(&d_key, mi * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&d_mlen, mi * sizeof(unsigned)) != cudaSuccess ||
-            cudaMalloc(&d_order, mi * sizeof(unsigned)) != cudaSuccess ||
-            cudaMalloc(&d_off, mi * sizeof(unsigned long long)) != cudaSuccess || cudaMalloc(&scratch, scratch_bytes) != cudaSuccess ||
-            cudaMallocHost(&h_stage, stage_bytes(mi)) != cudaSuccess || cudaMallocHost(&h_status, sizeof(FusedQueue)) != cudaSuccess)
+        if ((mk && (cudaMalloc(&sk_cache, mk * sk_pitch) != cudaSuccess || cudaMalloc(&pk_cache, mk * pk_pitch) != cudaSuccess)) ||
+            (mi && (cudaMalloc(&items, mi * C::ITEM_BYTES) != cudaSuccess || cudaMalloc(&best, mi * sizeof(unsigned)) != cudaSuccess ||
+                    cudaMalloc(&locks, mi * sizeof(unsigned)) != cudaSuccess ||
+                    cudaMalloc(&next_nonce, mi * sizeof(unsigned)) != cudaSuccess ||
+                    cudaMalloc(&inflight, mi * sizeof(unsigned)) != cudaSuccess ||
+                    cudaMalloc(&d_key, mi * sizeof(unsigned)) != cudaSuccess ||
+                    cudaMalloc(&d_mlen, mi * sizeof(unsigned)) != cudaSuccess ||
+                    cudaMalloc(&d_order, mi * sizeof(unsigned)) != cudaSuccess ||
+                    cudaMalloc(&d_off, mi * sizeof(unsigned long long)) != cudaSuccess ||
+                    cudaMalloc(&scratch, scratch_bytes) != cudaSuccess)) ||
+            cudaMalloc(&q, sizeof(FusedQueue)) != cudaSuccess || cudaMallocHost(&h_stage, stage_bytes(mi)) != cudaSuccess ||
+            cudaMallocHost(&h_status, sizeof(FusedQueue)) != cudaSuccess)
             return CUDIL_ERR_CUDA;
         std::memset(h_status, 0, sizeof(FusedQueue));
         return cudaMemset(q, 0, sizeof(FusedQueue)) == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
@@ -115,8 +123,10 @@ struct EngineImpl : EngineBase {
     ~EngineImpl() override {
         if (g_sign) cudaGraphExecDestroy(g_sign);
         if (g_verify) cudaGraphExecDestroy(g_verify);
-        cudaFree(sk_cache);
-        cudaFree(pk_cache);
+        if (owns_cache) {
+            cudaFree(sk_cache);
+            cudaFree(pk_cache);
+        }
         cudaFree(items);
         cudaFree(best);
         cudaFree(locks);
@@ -133,8 +143,26 @@ struct EngineImpl : EngineBase {
     }
 
     // ------------------------------------------------------------ key caches
+    // Use another engine's key caches (same parameter set); its caches must outlive this engine.
+    int attach_keys(const EngineBase *src) {
+        if (!src || src->mode != MODE || src == this) return CUDIL_ERR_INVALID;
+        if (owns_cache) {
+            cudaFree(sk_cache);
+            cudaFree(pk_cache);
+        }
+        owns_cache = false;
+        sk_cache = src->sk_cache;
+        pk_cache = src->pk_cache;
+        n_sk = src->n_sk;
+        n_pk = src->n_pk;
+        max_keys = src->max_keys;
+        g_sign_key[0] = nullptr;  // re-capture graphs with the new cache pointers
+        g_verify_key[0] = nullptr;
+        return CUDIL_OK;
+    }
+
     int set_secret_keys(const uint8_t *d_sk, size_t nkeys, cudaStream_t st) {
-        if (!d_sk || nkeys == 0 || nkeys > max_keys) return CUDIL_ERR_INVALID;
+        if (!d_sk || nkeys == 0 || nkeys > max_keys || !owns_cache) return CUDIL_ERR_INVALID;
         const int nn = (int)nkeys;
         CUDIL_LAUNCH(KID_CACHE_SK, st,
                      k_cache_sk<MODE><<<blocks_for(nkeys * (PM::L + 2 * PM::K + 1) * 16), kBlock, 0, st>>>(d_sk, sk_cache, sk_pitch, nn));
@@ -147,7 +175,7 @@ struct EngineImpl : EngineBase {
     }
 
     int set_public_keys(const uint8_t *d_pk, size_t nkeys, cudaStream_t st) {
-        if (!d_pk || nkeys == 0 || nkeys > max_keys) return CUDIL_ERR_INVALID;
+        if (!d_pk || nkeys == 0 || nkeys > max_keys || !owns_cache) return CUDIL_ERR_INVALID;
         const int nn = (int)nkeys;
         CUDIL_LAUNCH(KID_CACHE_PK, st, k_cache_pk_tr<MODE><<<blocks_for(nkeys), kBlock, 0, st>>>(d_pk, pk_cache, pk_pitch, nn));
         CUDIL_CK_LAUNCH();

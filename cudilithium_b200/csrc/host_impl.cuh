@@ -74,12 +74,12 @@ struct Impl {
     }
 
     // ---------------------------------------------------------------- sign
-    static int sign_setup(const uint8_t *m, size_t m_pitch, size_t mlen, const uint8_t *sk, size_t sk_pitch,
-                          uint8_t *pool, size_t sp, size_t n, cudaStream_t st, cudaMemcpyKind in_kind) {
+    static int sign_setup(const uint8_t *m, size_t m_pitch, size_t mlen, const uint32_t *mlens, const uint8_t *sk,
+                          size_t sk_pitch, uint8_t *pool, size_t sp, size_t n, cudaStream_t st, cudaMemcpyKind in_kind) {
         const int nn = (int)n;
         if (mlen) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::SG_MSG, sp, m, m_pitch, mlen, n, in_kind, st));
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::SG_SK, sp, sk, sk_pitch, PM::SK_BYTES, n, in_kind, st));
-        CUDIL_LAUNCH(KID_SIGN_PREHASH, st, k_sign_prehash<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, sp, mlen, nn));
+        CUDIL_LAUNCH(KID_SIGN_PREHASH, st, k_sign_prehash<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, sp, mlen, mlens, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_EXPAND_A, st, k_expand_a<MODE><<<blocks_for(n * K * L), kBlock, 0, st>>>(pool, sp, LY::SG_SK + PM::SK_RHO, LY::sg_mat(mlen), nn));
         CUDIL_CK_LAUNCH();
@@ -102,10 +102,12 @@ struct Impl {
         return CUDIL_OK;
     }
 
+    // mlens: optional device array of per-item message lengths (each <= mlen; rows of m hold the
+    // message in their first mlens[i] bytes); nullptr = every message is mlen bytes.
     static int sign(uint8_t *sig, size_t sig_pitch, size_t *siglen, const uint8_t *m, size_t m_pitch, size_t mlen,
                     const uint8_t *sk, size_t sk_pitch, uint8_t *pool, size_t sp, uint8_t *tpool, size_t tp,
                     cudil_task_lut *lut, size_t T, size_t n, cudaStream_t st, cudaMemcpyKind in_kind,
-                    cudaMemcpyKind out_kind) {
+                    cudaMemcpyKind out_kind, const uint32_t *mlens = nullptr) {
         if (siglen) *siglen = PM::SIG_BYTES;
         if (n == 0) return CUDIL_OK;
         if (!sig || !sk || (!m && mlen) || !pool || !tpool || !lut || T == 0 || n > 65536) return CUDIL_ERR_INVALID;
@@ -115,7 +117,7 @@ struct Impl {
         if (!lut->sign_lut || lut->sign_lut_len != n || !lut->h_exec_lut || !lut->h_done_lut || !lut->h_copy_lut ||
             !lut->d_exec_lut || !lut->d_done_lut || !lut->d_copy_lut)
             return CUDIL_ERR_INVALID;
-        int rc = sign_setup(m, m_pitch, mlen, sk, sk_pitch, pool, sp, n, st, in_kind);
+        int rc = sign_setup(m, m_pitch, mlen, mlens, sk, sk_pitch, pool, sp, n, st, in_kind);
         if (rc) return rc;
 
         cudil_sign_lut_element *sl = lut->sign_lut;
@@ -175,7 +177,7 @@ struct Impl {
     // ---------------------------------------------------------------- verify
     static int verify(int *ret, const uint8_t *sig, size_t sig_pitch, size_t siglen, const uint8_t *m, size_t m_pitch,
                       size_t mlen, const uint8_t *pk, size_t pk_pitch, uint8_t *pool, size_t pitch, size_t n,
-                      cudaStream_t st, cudaMemcpyKind in_kind, cudaMemcpyKind out_kind) {
+                      cudaStream_t st, cudaMemcpyKind in_kind, cudaMemcpyKind out_kind, const uint32_t *mlens = nullptr) {
         if (n == 0) return CUDIL_OK;
         if (!ret) return CUDIL_ERR_INVALID;
         if (siglen != (size_t)PM::SIG_BYTES) {
@@ -193,7 +195,7 @@ struct Impl {
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::VF_SIG, pitch, sig, sig_pitch, PM::SIG_BYTES, n, in_kind, st));
         if (mlen) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::VF_TRM + SEEDBYTES, pitch, m, m_pitch, mlen, n, in_kind, st));
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::VF_PK, pitch, pk, pk_pitch, PM::PK_BYTES, n, in_kind, st));
-        CUDIL_LAUNCH(KID_VERIFY_PREPARE, st, k_verify_prepare<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, mlen, nn));
+        CUDIL_LAUNCH(KID_VERIFY_PREPARE, st, k_verify_prepare<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, mlen, mlens, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_EXPAND_A, st, k_expand_a<MODE><<<blocks_for(n * K * L), kBlock, 0, st>>>(pool, pitch, LY::VF_PK, LY::vf_mat(mlen), nn));
         CUDIL_CK_LAUNCH();

@@ -23,14 +23,16 @@ constexpr int kGroupsPerBlock = 8;      // 16-thread groups per 128-thread block
 // ------------------------------------------------------------------ per-item setup
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_sign_prehash(uint8_t *pool, size_t pitch, size_t mlen, int n) {
+__global__ void __launch_bounds__(kBlock) k_sign_prehash(uint8_t *pool, size_t pitch, size_t mlen, const uint32_t *mlens,
+                                                         int n) {
     using LY = Layout<MODE>;
     const int it = blockIdx.x * blockDim.x + threadIdx.x;
     if (it >= n) return;
     uint8_t *row = pool + (size_t)it * pitch;
+    const size_t ml = mlens ? (size_t)mlens[it] : mlen;  // per-item length (<= mlen) when given
     uint32_t al[25], ah[25];
-    TwoPart src{row + LY::SG_SK + P<MODE>::SK_TR, 4, row + LY::SG_MSG, (long long)mlen};
-    shake_absorb<SHAKE256_RATE>(al, ah, src, (long long)(SEEDBYTES + mlen));
+    TwoPart src{row + LY::SG_SK + P<MODE>::SK_TR, 4, row + LY::SG_MSG, (long long)ml};
+    shake_absorb<SHAKE256_RATE>(al, ah, src, (long long)(SEEDBYTES + ml));
     keccak_f1600(al, ah);
     uint2 mu[8];
 #pragma unroll

@@ -13,7 +13,8 @@
 namespace cudil {
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_verify_prepare(uint8_t *pool, size_t pitch, size_t mlen, int n) {
+__global__ void __launch_bounds__(kBlock) k_verify_prepare(uint8_t *pool, size_t pitch, size_t mlen, const uint32_t *mlens,
+                                                           int n) {
     using PM = P<MODE>;
     using LY = Layout<MODE>;
     constexpr int K = PM::K, OMEGA = PM::OMEGA;
@@ -53,9 +54,10 @@ __global__ void __launch_bounds__(kBlock) k_verify_prepare(uint8_t *pool, size_t
     uint2 *trm = reinterpret_cast<uint2 *>(row + LY::VF_TRM);
 #pragma unroll
     for (int w = 0; w < 4; ++w) trm[w] = make_uint2(al[w], ah[w]);
-    // mu = SHAKE256(tr' || m, 64)
-    AlignedBytes tm{row + LY::VF_TRM, (long long)(SEEDBYTES + mlen)};
-    shake_absorb<SHAKE256_RATE>(al, ah, tm, (long long)(SEEDBYTES + mlen));
+    // mu = SHAKE256(tr' || m, 64); per-item length (<= mlen) when given
+    const size_t ml = mlens ? (size_t)mlens[it] : mlen;
+    AlignedBytes tm{row + LY::VF_TRM, (long long)(SEEDBYTES + ml)};
+    shake_absorb<SHAKE256_RATE>(al, ah, tm, (long long)(SEEDBYTES + ml));
     keccak_f1600(al, ah);
     uint2 *mu = reinterpret_cast<uint2 *>(row + LY::vf_mu(mlen));
 #pragma unroll

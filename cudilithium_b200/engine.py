@@ -78,6 +78,11 @@ class Engine:
         n = d_sk.numel() // self.params.sk_bytes
         check(lib.cudil_engine_set_secret_keys(self.h, d_sk.data_ptr(), n, _sp(stream)), "set_secret_keys")
 
+    def attach_keys(self, src: "Engine"):
+        """Share src's key caches (same parameter set); src must outlive this engine."""
+        check(lib.cudil_engine_attach_keys(self.h, src.h), "attach_keys")
+        self._cache_owner = src
+
     def set_public_keys(self, d_pk: torch.Tensor, stream=None):
         n = d_pk.numel() // self.params.pk_bytes
         check(lib.cudil_engine_set_public_keys(self.h, d_pk.data_ptr(), n, _sp(stream)), "set_public_keys")

@@ -109,6 +109,18 @@ int cudil_verify_dev(int mode, int *d_ret, const uint8_t *d_sig, size_t sig_pitc
                      size_t m_pitch, size_t mlen, const uint8_t *d_pk, uint8_t *d_verify_pool,
                      size_t verify_pool_pitch, size_t batch_size, void *stream);
 
+/* Per-item message lengths (device-resident variants; extends the reference API, which has one
+ * mlen per call, include/api.cuh:51-63): row i of d_m (m_pitch apart) holds a message of
+ * d_mlens[i] <= max_mlen bytes; pools are sized for max_mlen. */
+int cudil_sign_dev_varlen(int mode, uint8_t *d_sig, size_t sig_pitch, const uint8_t *d_m, size_t m_pitch,
+                          const uint32_t *d_mlens, size_t max_mlen, const uint8_t *d_sk, uint8_t *d_sign_pool,
+                          size_t sign_pool_pitch, uint8_t *d_temp_pool, size_t temp_pool_pitch, cudil_task_lut *lut,
+                          size_t exec_threshold, size_t batch_size, void *stream);
+int cudil_verify_dev_varlen(int mode, int *d_ret, const uint8_t *d_sig, size_t sig_pitch, size_t siglen,
+                            const uint8_t *d_m, size_t m_pitch, const uint32_t *d_mlens, size_t max_mlen,
+                            const uint8_t *d_pk, uint8_t *d_verify_pool, size_t verify_pool_pitch, size_t batch_size,
+                            void *stream);
+
 /* Verification without any device allocation, for callers that may not allocate device memory
  * where they verify (budgeted or pre-reserved device memory, latency-critical threads that must
  * not hit cudaMalloc/cudaFree, hosts that own every allocation).  No counterpart in the
@@ -156,6 +168,9 @@ int cudil_engine_create(cudil_engine **out, int mode, size_t max_keys, size_t ma
 int cudil_engine_destroy(cudil_engine *e);
 size_t cudil_engine_device_bytes(const cudil_engine *e);
 int cudil_engine_set_secret_keys(cudil_engine *e, const uint8_t *d_sk, size_t nkeys, void *stream);
+/* Share src's key caches (same parameter set; src must outlive e).  An engine created with
+ * max_keys = 0 owns no caches and must attach before signing or verifying. */
+int cudil_engine_attach_keys(cudil_engine *e, const cudil_engine *src);
 int cudil_engine_set_public_keys(cudil_engine *e, const uint8_t *d_pk, size_t nkeys, void *stream);
 int cudil_engine_sign(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
                       const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
@@ -177,6 +192,63 @@ int cudil_engine_set_spec_slots(cudil_engine *e, unsigned spec_slots);
  * Keccak phases, NTT phases and in total, and the number of block iterations. */
 int cudil_engine_last_phases(const cudil_engine *e, unsigned long long cycles[4], unsigned *iterations);
 int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks);
+
+/* ---------------------------------------------------------------------------------------------
+ * Request server: continuous batching over a mixed request stream (no reference counterpart; the
+ * reference only has the blocking batch calls above).
+ *
+ * cudil_serve_trace replays an open-loop trace in real time on the current device.  Request i
+ * becomes visible arrival_s seconds after the start and queues in the FIFO of its (parameter set,
+ * operation) lane.  Each lane owns up to slots_per_lane batch slots (stream + device buffers); a
+ * free slot takes everything queued in its lane (at most max_batch) as one batch, so batches of
+ * every lane overlap on the device while new requests queue.  Slots are created only while the
+ * device-memory estimate stays within device_budget_bytes (0 = unlimited); every lane in use
+ * needs one (else CUDIL_ERR_BUDGET).
+ * path 0: fused engines sharing one resident key cache per parameter set (sk and pk of every key
+ *         expanded once before the replay starts, outside the timed region);
+ * path 1: the plain stage-by-stage calls (key material expanded per batch).
+ * Messages are msgs[msg_off .. msg_off + mlen) (mlen <= max_mlen); verify requests read
+ * sigs[sig_off .. + sig_bytes).  Results: status 0 / -1 (verify), done_s = host time the request's
+ * batch completed; signatures go to sig_out + i * sig_out_pitch (NULL: not returned).
+ * Returns CUDIL_OK or the first error. */
+typedef struct {
+    double arrival_s;
+    int32_t mode; /* 2, 3 or 5 */
+    int32_t op;   /* 0 sign, 1 verify */
+    uint32_t key; /* index into the parameter set's key array */
+    uint32_t mlen;
+    unsigned long long msg_off, sig_off;
+} cudil_request;
+
+typedef struct {
+    double done_s;
+    int32_t status;
+    uint32_t batch_size; /* size of the batch that served the request */
+} cudil_request_result;
+
+typedef struct {
+    size_t device_budget_bytes;
+    int32_t path;           /* 0 fused, 1 plain */
+    int32_t slots_per_lane; /* >= 1 */
+    int32_t max_batch;      /* >= 1 */
+    int32_t engine_threads; /* fused: threads per block (0 = default) */
+    int32_t engine_spec_slots;    /* fused: signer speculation target (0 = default) */
+    int32_t plain_exec_threshold; /* plain: signing attempts per round (>= 1) */
+    uint32_t max_mlen;
+    uint32_t reserved;
+} cudil_serve_config;
+
+typedef struct {
+    double wall_s;       /* first arrival window start to last completion */
+    size_t batches;      /* batches launched */
+    size_t slots;        /* batch slots created within the budget */
+    size_t device_bytes; /* device-memory estimate of caches + slots */
+} cudil_serve_stats;
+
+int cudil_serve_trace(const cudil_serve_config *cfg, const uint8_t *const sk[3], const uint8_t *const pk[3],
+                      const size_t nkeys[3], const cudil_request *reqs, size_t nreq, const uint8_t *msgs,
+                      const uint8_t *sigs, uint8_t *sig_out, size_t sig_out_pitch, cudil_request_result *results,
+                      cudil_serve_stats *stats);
 
 /* Peak of the 32-bit LOP3/funnel-shift mix Keccak-f[1600] issues: launches `blocks` x 256 threads
  * doing `iters` x 32 ALU operations each; *ops_per_launch receives the operation count. */
