@@ -418,6 +418,7 @@ def run_gpu(args) -> dict | None:
     torch.cuda.empty_cache()
     if not args.quick:
         result["configs"] = run_configs(args, torch, np, lib, _lib, dev, spp, rank)
+        result["configs"]["serve_mixed"] = run_serve(args, np)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -616,6 +617,62 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank) -> dict:
     return out
 
 
+def run_serve(args, np) -> dict:
+    """Serving loop: open-loop Poisson stream mixing Dilithium2/3/5 (60/25/15), 70% verify / 30%
+    sign, resident seeded keys per parameter set, message lengths log-uniform 32 B - 4 KiB, fixed
+    device-memory budget.  Per path (fused engines with resident key caches / plain stage-by-stage
+    calls): saturation throughput (every request queued at t = 0), then Poisson arrivals at
+    fractions of it with p50/p99 latency (arrival to completion seen by the host)."""
+    import torch
+
+    from cudilithium_b200.serve import Trace, make_keys, poisson_trace, serve, summary
+    nkeys = args.serve_keys
+    t0 = time.time()
+    keys = make_keys({2: nkeys, 3: nkeys, 5: nkeys})
+    base = poisson_trace(keys, rate=float("inf"), n=args.serve_requests, seed=11)
+    log(f"[serve] keys + trace of {len(base.reqs)} requests in {time.time() - t0:.1f}s")
+    torch.cuda.empty_cache()
+    rng = np.random.default_rng(12)
+    budget = int(args.serve_budget_gib * 2**30)
+    out = {"workload": f"open-loop Poisson, Dilithium2/3/5 = 60/25/15, 70% verify / 30% sign, {nkeys} resident "
+                       f"keys per parameter set, mlen log-uniform 32 B - 4 KiB, {len(base.reqs)} distinct requests "
+                       f"repeated over a {args.serve_seconds} s arrival window per point, device budget "
+                       f"{args.serve_budget_gib} GiB",
+           "budget_bytes": budget, "latency": "arrival to completion observed by the host, ms"}
+    def tiled(n, rate):
+        # the unique requests repeated (same messages and signatures) up to n, arrivals redrawn
+        r = np.resize(base.reqs, n)
+        r["arrival_s"] = 0.0 if math.isinf(rate) else np.cumsum(rng.exponential(1.0 / rate, n))
+        return Trace(r, base.msgs, base.sigs, np.resize(base.expect, n), rate)
+
+    for path, name in ((0, "fused"), (1, "plain")):
+        cfgkw = dict(path=path, budget_bytes=budget, slots_per_lane=args.serve_slots, max_batch=args.serve_max_batch)
+        tr = tiled(max(len(base.reqs), int(args.serve_seconds * 4e6)), float("inf"))
+        res, _, st = serve(tr, keys, want_sigs=False, **cfgkw)
+        ok = bool(np.array_equal(res["status"][tr.reqs["op"] == 1], tr.expect[tr.reqs["op"] == 1]))
+        sat = summary(tr, res, st)
+        peak = sat["throughput_per_s"]
+        points = []
+        for f in args.serve_fracs:
+            rate = f * peak
+            tr = tiled(max(20_000, int(rate * args.serve_seconds)), rate)
+            res, _, st = serve(tr, keys, want_sigs=False, **cfgkw)
+            ok &= bool(np.array_equal(res["status"][tr.reqs["op"] == 1], tr.expect[tr.reqs["op"] == 1]))
+            sm = summary(tr, res, st)
+            points.append({"offered_frac_of_peak": f, "offered_per_s": rate, "achieved_per_s": sm["throughput_per_s"],
+                           "achieved_frac_of_peak": sm["throughput_per_s"] / peak, "p50_ms": sm["p50_ms"],
+                           "p99_ms": sm["p99_ms"], "mean_batch": sm["mean_batch"], "lanes": sm["lanes"]})
+            log(f"[serve] {name} rate {rate:,.0f}/s -> {sm['throughput_per_s']:,.0f}/s p50 {sm['p50_ms']:.2f} ms "
+                f"p99 {sm['p99_ms']:.2f} ms")
+        out[name] = {"peak_per_s": peak, "saturation": {k: sat[k] for k in ("p50_ms", "p99_ms", "mean_batch", "slots",
+                                                                             "device_bytes", "batches", "wall_s",
+                                                                             "slot_time_s")},
+                     "points": points, "verify_status_exact": ok}
+        log(f"[serve] {name} saturation {peak:,.0f} requests/s, slots {sat['slots']}")
+    out["fused_over_plain_peak"] = out["fused"]["peak_per_s"] / out["plain"]["peak_per_s"]
+    return out
+
+
 def ctypes_byref(x):
     import ctypes
     return ctypes.byref(x)
@@ -722,8 +779,16 @@ def main():
     ap.add_argument("--spec-slots", type=int, default=0, help="fused signer attempts in flight (0 = tuned default)")
     ap.add_argument("--quick", action="store_true", help="headline only (skip configs 1-4)")
     ap.add_argument("--workload", default="headline",
-                    choices=["headline", "fused-sign", "fused-verify", "ntt", "plain-sign"],
+                    choices=["headline", "serve", "fused-sign", "fused-verify", "ntt", "plain-sign"],
                     help="headline = the bench line; the others are small self-checking cases for ncu")
+    ap.add_argument("--serve-keys", type=int, default=4096, help="resident keys per parameter set (serving)")
+    ap.add_argument("--serve-requests", type=int, default=200_000, help="distinct requests of the serving trace")
+    ap.add_argument("--serve-seconds", type=float, default=1.0, help="arrival window per serving point")
+    ap.add_argument("--serve-fracs", type=float, nargs="+", default=[0.5, 0.8, 0.9],
+                    help="offered load as fractions of the saturation throughput")
+    ap.add_argument("--serve-slots", type=int, default=2, help="batch slots per (parameter set, op) lane")
+    ap.add_argument("--serve-max-batch", type=int, default=8192)
+    ap.add_argument("--serve-budget-gib", type=float, default=48.0, help="device-memory budget of the server")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-sample", type=int, default=4000)
     ap.add_argument("--no-cpu", action="store_true")
@@ -733,6 +798,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         res = run_reference(args)
+    elif args.workload == "serve":
+        import numpy as np
+        res = {"configs": {"serve_mixed": run_serve(args, np)}}
     elif args.workload != "headline":
         res = run_profile_case(args)
     else:

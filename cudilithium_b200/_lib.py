@@ -66,7 +66,8 @@ class cudil_serve_config(ctypes.Structure):
 
 class cudil_serve_stats(ctypes.Structure):
     _fields_ = [("wall_s", ctypes.c_double), ("batches", c_size_t), ("slots", c_size_t),
-                ("device_bytes", c_size_t)]
+                ("device_bytes", c_size_t), ("host_stage_s", ctypes.c_double), ("device_wait_s", ctypes.c_double),
+                ("host_post_s", ctypes.c_double)]
 
 
 # Every symbol the public header declares, with its ctypes signature.

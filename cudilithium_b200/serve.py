@@ -173,7 +173,8 @@ def serve(tr: Trace, keys: Keys, path: int = 0, budget_bytes: int = 0, slots_per
                                res.ctypes.data, ctypes.byref(st))
     check(rc, "cudil_serve_trace")
     return res, sig_out, {"wall_s": st.wall_s, "batches": st.batches, "slots": st.slots,
-                          "device_bytes": st.device_bytes}
+                          "device_bytes": st.device_bytes, "host_stage_s": st.host_stage_s,
+                          "device_wait_s": st.device_wait_s, "host_post_s": st.host_post_s}
 
 
 def summary(tr: Trace, res: np.ndarray, stats: dict) -> dict:
@@ -185,7 +186,8 @@ def summary(tr: Trace, res: np.ndarray, stats: dict) -> dict:
            "p50_ms": float(np.percentile(lat, 50)) if len(lat) else 0.0,
            "p99_ms": float(np.percentile(lat, 99)) if len(lat) else 0.0,
            "mean_batch": float(res["batch_size"].mean()) if len(res) else 0.0,
-           "batches": stats["batches"], "slots": stats["slots"], "device_bytes": stats["device_bytes"], "lanes": {}}
+           "batches": stats["batches"], "slots": stats["slots"], "device_bytes": stats["device_bytes"],
+           "slot_time_s": {k: stats[k] for k in ("host_stage_s", "device_wait_s", "host_post_s")}, "lanes": {}}
     for m in MODES:
         for op, name in ((SIGN, "sign"), (VERIFY, "verify")):
             sel = (tr.reqs["mode"] == m) & (tr.reqs["op"] == op)

@@ -243,6 +243,9 @@ typedef struct {
     size_t batches;      /* batches launched */
     size_t slots;        /* batch slots created within the budget */
     size_t device_bytes; /* device-memory estimate of caches + slots */
+    /* summed over slots: staging requests into pinned buffers, first copy / launch to stream
+     * completion (H2D + kernels + D2H, including waits behind other slots), result write-back */
+    double host_stage_s, device_wait_s, host_post_s;
 } cudil_serve_stats;
 
 int cudil_serve_trace(const cudil_serve_config *cfg, const uint8_t *const sk[3], const uint8_t *const pk[3],
