@@ -746,6 +746,8 @@ def run_profile_case(args) -> dict:
         torch.cuda.synchronize()
         return {"workload": "plain-sign", "batch": B}
     es = Engine(mode, B, B, threads=args.engine_threads)
+    if args.sign_kernel >= 0:
+        es.set_sign_kernel(args.sign_kernel)
     if args.spec_slots:
         es.set_spec_slots(args.spec_slots)
     es.set_secret_keys(sk, stream=spp)
@@ -777,6 +779,8 @@ def main():
                     help="exec-slot counts tried for the plain path (the fastest is used)")
     ap.add_argument("--engine-threads", type=int, default=0, help="fused engine block size (0 = tuned default)")
     ap.add_argument("--spec-slots", type=int, default=0, help="fused signer attempts in flight (0 = tuned default)")
+    ap.add_argument("--sign-kernel", type=int, default=-1,
+                    help="fused signer kernel: 0 phased, 1 async 256/64, 2 async 512/128 (-1 = tuned default)")
     ap.add_argument("--quick", action="store_true", help="headline only (skip configs 1-4)")
     ap.add_argument("--workload", default="headline",
                     choices=["headline", "serve", "fused-sign", "fused-verify", "ntt", "plain-sign"],

@@ -1,5 +1,5 @@
-"""Autotuner for the fused engine: picks the block size and the signer's per-block speculation
-target for each parameter set by timing real signing batches, and caches the result as JSON
+"""Autotuner for the fused engine: picks the signer kernel (phased or asynchronous), the block
+size and the per-block speculation target for each parameter set by timing real signing batches, and caches the result as JSON
 (``cudilithium_b200/tuned.json``, keyed by GPU name).
 
     python -m cudilithium_b200.autotune [--modes 2 3 5] [--batch 16384]
@@ -17,10 +17,13 @@ from pathlib import Path
 TUNED_PATH = Path(__file__).resolve().parent / "tuned.json"
 # measured on B200 (Dilithium2, 10000 and 65536 single-use keys): 256 threads per block and a
 # per-block target of 32 attempts in flight gave the highest signing throughput
-DEFAULTS = {2: {"threads": 256, "spec_slots": 32}, 3: {"threads": 256, "spec_slots": 32},
-            5: {"threads": 256, "spec_slots": 32}}
+DEFAULTS = {2: {"threads": 256, "spec_slots": 32, "sign_kernel": 0},
+            3: {"threads": 256, "spec_slots": 32, "sign_kernel": 0},
+            5: {"threads": 256, "spec_slots": 32, "sign_kernel": 0}}
 THREADS = (128, 256)
 SPEC = (16, 32, 64, 128)
+# asynchronous signer variants (kernel, speculation target = its slot count)
+ASYNC = ((2, 128), (3, 160))
 
 
 def _gpu_name() -> str:
@@ -64,7 +67,9 @@ def tune_mode(mode: int, batch: int, reps: int = 3) -> dict:
     for t in THREADS:
         e = Engine(mode, batch, batch, threads=t)
         e.set_secret_keys(sk, stream=spp)
-        for s in SPEC:
+        cands = [(0, s) for s in SPEC] + ([(v, s) for v, s in ASYNC] if t == THREADS[-1] else [])
+        for kern, s in cands:
+            e.set_sign_kernel(kern)
             e.set_spec_slots(s)
             e.sign(sig, m, offs, lens, keys, stream=spp)
             torch.cuda.synchronize()
@@ -78,10 +83,10 @@ def tune_mode(mode: int, batch: int, reps: int = 3) -> dict:
             b.record()
             torch.cuda.synchronize()
             ms = a.elapsed_time(b) / reps
-            results.append({"threads": t, "spec_slots": s, "ms": ms, "sign_per_s": batch / (ms / 1e3)})
+            results.append({"threads": t, "spec_slots": s, "sign_kernel": kern, "ms": ms, "sign_per_s": batch / (ms / 1e3)})
         e.close()
     best = min(results, key=lambda r: r["ms"])
-    return {"threads": best["threads"], "spec_slots": best["spec_slots"], "batch": batch,
+    return {"threads": best["threads"], "spec_slots": best["spec_slots"], "sign_kernel": best["sign_kernel"], "batch": batch,
             "sign_per_s": best["sign_per_s"], "candidates": results, "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
 
 
@@ -101,7 +106,7 @@ def main():
     for mode in args.modes:
         r = tune_mode(mode, args.batch)
         entry[str(mode)] = r
-        print(json.dumps({"mode": mode, "threads": r["threads"], "spec_slots": r["spec_slots"],
+        print(json.dumps({"mode": mode, "threads": r["threads"], "spec_slots": r["spec_slots"], "sign_kernel": r["sign_kernel"],
                           "sign_per_s": round(r["sign_per_s"])}), flush=True)
     TUNED_PATH.write_text(json.dumps(data, indent=1))
 

@@ -177,6 +177,35 @@ __device__ __forceinline__ void unpack_z_strided(int32_t (&x)[16], const uint8_t
     for (int i = 0; i < 16; ++i) x[i] = Params<MODE>::GAMMA1 - (int32_t)get_bits(packed, (t + 16 * i) * ZB, ZB);
 }
 
+// z coefficients a[16 t + i] (the contiguous slice of group thread t) from a packed (gamma1 - z)
+// polynomial whose start is 4-byte aligned: the slice is 16 * Z_BITS / 32 whole words, read as
+// 32-bit loads and split with funnel shifts.
+template <int MODE>
+__device__ __forceinline__ void unpack_z_contig(int32_t (&x)[16], const uint8_t *packed, int t) {
+    constexpr int ZB = P<MODE>::Z_BITS, NWD = ZB / 2;
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(packed) + NWD * t;
+    uint32_t v[NWD + 1];
+#pragma unroll
+    for (int k = 0; k < NWD; ++k) v[k] = w[k];
+    v[NWD] = 0u;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int bit = i * ZB, wi = bit >> 5, sh = bit & 31;
+        const uint32_t r = __funnelshift_r(v[wi], v[wi + 1], sh) & ((1u << ZB) - 1u);
+        x[i] = Params<MODE>::GAMMA1 - (int32_t)r;
+    }
+}
+
+// Inverse of strided_to_contig: y[i] = a[16 t + i] -> x[i] = a[t + 16 i].
+__device__ __forceinline__ void contig_to_strided(const Group &g, const int32_t (&y)[16], int32_t (&x)[16]) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) g.sm[17 * g.t + i] = y[i];
+    __syncwarp(g.gmask);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = g.sm[g.t + 17 * i];
+    __syncwarp(g.gmask);
+}
+
 // c coefficients a[t + 16 i] from the challenge masks (occupied bits, negative bits).
 __device__ __forceinline__ void challenge_strided(int32_t (&x)[16], const uint32_t *masks, int t) {
 #pragma unroll

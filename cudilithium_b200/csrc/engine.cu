@@ -130,11 +130,22 @@ int cudil_engine_attach_keys(cudil_engine *e, const cudil_engine *src) {
 
 int cudil_engine_set_spec_slots(cudil_engine *e, unsigned spec_slots) { CUDIL_ENGINE_DISPATCH(e, set_spec_slots(spec_slots)); }
 
+int cudil_engine_last_jobs(const cudil_engine *e, unsigned long long out[12]) {
+    if (!e || !e->impl || !out) return CUDIL_ERR_INVALID;
+    for (int i = 0; i < 12; ++i) out[i] = e->impl->h_status->jobs[i];
+    return CUDIL_OK;
+}
+
+int cudil_engine_set_sign_kernel(cudil_engine *e, int variant) { CUDIL_ENGINE_DISPATCH(e, set_sign_kernel(variant)); }
+
 int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks) {
     if (!e || !e->impl) return CUDIL_ERR_INVALID;
     if (mode) *mode = e->impl->mode;
     if (threads) *threads = e->impl->threads;
-    if (sign_blocks) *sign_blocks = e->impl->sign_grid;
+    if (sign_blocks) {
+        const EngineBase *b = e->impl;
+        *sign_blocks = b->sign_kernel == 0 ? b->sign_grid : b->async_grid[b->sign_kernel - 1];
+    }
     if (verify_blocks) *verify_blocks = e->impl->verify_grid;
     return CUDIL_OK;
 }

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "fused_kernels.cuh"
+#include "fused_sign_async.cuh"
 #include "host_impl.cuh"
 #include "profiling.cuh"
 
@@ -38,6 +39,13 @@ struct EngineBase {
     size_t scratch_bytes = 0;
     int sign_grid = 0, verify_grid = 0, prehash_grid = 0;
     size_t sign_smem = 0, verify_smem = 0;
+    // signer kernel: 0 = phased k_fused_sign (block-wide Keccak / NTT phases); 1..4 = asynchronous
+    // k_fused_sign_async with (threads, slots) per block of (256, 64), (512, 128), (640, 160),
+    // (768, 192)
+    int sign_kernel = 0;
+    static constexpr int kAsyncVariants = 4;  // (threads, slots) = (256, 64), (512, 128), (640, 160), (768, 192)
+    int async_grid[kAsyncVariants] = {0, 0, 0, 0};
+    size_t async_smem[kAsyncVariants] = {0, 0, 0, 0};
     // instantiated graphs, keyed by the output / message buffers they were captured with
     cudaGraphExec_t g_sign = nullptr, g_verify = nullptr;
     const void *g_sign_key[2] = {nullptr, nullptr}, *g_verify_key[2] = {nullptr, nullptr};
@@ -64,13 +72,35 @@ struct EngineImpl : EngineBase {
     }
 
     // Device bytes the engine needs (the admission budget checks this before allocating).
-    static size_t required_bytes(size_t max_keys, size_t max_items, int threads, int sign_grid, int verify_grid) {
+    size_t required_bytes(size_t max_keys, size_t max_items) const {
         return max_keys * (align256(C::SK_ROW) + align256(C::PK_ROW)) + max_items * (C::ITEM_BYTES + 4 * sizeof(unsigned)) +
-               stage_bytes(max_items) + sizeof(FusedQueue) + scratch_for(max_items, threads, sign_grid, verify_grid);
+               stage_bytes(max_items) + sizeof(FusedQueue) + scratch_for(max_items);
     }
-    static size_t scratch_for(size_t max_items, int threads, int sign_grid, int verify_grid) {
+    // attempt slots of the largest signer variant, or the verifier's per-signature slots
+    size_t scratch_for(size_t max_items) const {
         if (max_items == 0) return 0;
-        return std::max((size_t)sign_grid * 2 * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
+        size_t b = std::max((size_t)sign_grid * 2 * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
+        static constexpr int slots[kAsyncVariants] = {64, 128, 160, 192};
+        for (int v = 0; v < kAsyncVariants; ++v) b = std::max(b, (size_t)async_grid[v] * slots[v] * C::SLOT);
+        return b;
+    }
+
+    template <int T, int S>
+    int configure_async_one(int v) {
+        async_smem[v] = AsyncSignSmem<MODE, T, S>::BYTES;
+        if (cudaFuncSetAttribute(k_fused_sign_async<MODE, T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)async_smem[v]) != cudaSuccess)
+            return CUDIL_ERR_CUDA;
+        async_grid[v] = grid_for<T>((const void *)k_fused_sign_async<MODE, T, S>, async_smem[v], sm_count);
+        return async_grid[v] > 0 ? CUDIL_OK : CUDIL_ERR_CUDA;
+    }
+
+    int configure_async() {
+        int rc = configure_async_one<256, 64>(0);
+        if (!rc) rc = configure_async_one<512, 128>(1);
+        if (!rc) rc = configure_async_one<640, 160>(2);
+        if (!rc) rc = configure_async_one<768, 192>(3);
+        return rc;
     }
 
     template <int T>
@@ -96,12 +126,14 @@ struct EngineImpl : EngineBase {
         if (cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return CUDIL_ERR_CUDA;
         int rc = (threads == 128) ? configure<128>() : (threads == 256 ? configure<256>() : CUDIL_ERR_INVALID);
         if (rc) return rc;
+        rc = configure_async();
+        if (rc) return rc;
         prehash_grid = (int)std::min<size_t>((mi + kBlock - 1) / kBlock, (size_t)sm_count * 8);
-        device_bytes = required_bytes(mk, mi, threads, sign_grid, verify_grid);
+        device_bytes = required_bytes(mk, mi);
         if (budget && device_bytes > budget) return CUDIL_ERR_BUDGET;
         sk_pitch = align256(C::SK_ROW);
         pk_pitch = align256(C::PK_ROW);
-        scratch_bytes = scratch_for(mi, threads, sign_grid, verify_grid);
+        scratch_bytes = scratch_for(mi);
         spec_slots = (unsigned)threads;
         if ((mk && (cudaMalloc(&sk_cache, mk * sk_pitch) != cudaSuccess || cudaMalloc(&pk_cache, mk * pk_pitch) != cudaSuccess)) ||
             (mi && (cudaMalloc(&items, mi * C::ITEM_BYTES) != cudaSuccess || cudaMalloc(&best, mi * sizeof(unsigned)) != cudaSuccess ||
@@ -227,7 +259,16 @@ struct EngineImpl : EngineBase {
         k_fused_prehash<MODE><<<prehash_grid, kBlock, 0, st>>>(sk_cache, sk_pitch, mr, items, q);
         FusedSignArgs a{sk_cache, sk_pitch, d_key, items, d_sig, (size_t)PM::SIG_BYTES, scratch, q, best, locks, next_nonce,
                         inflight, spec_slots};
-        k_fused_sign<MODE, T><<<sign_grid, T, sign_smem, st>>>(a);
+        if (sign_kernel == 1)
+            k_fused_sign_async<MODE, 256, 64><<<async_grid[0], 256, async_smem[0], st>>>(a);
+        else if (sign_kernel == 2)
+            k_fused_sign_async<MODE, 512, 128><<<async_grid[1], 512, async_smem[1], st>>>(a);
+        else if (sign_kernel == 3)
+            k_fused_sign_async<MODE, 640, 160><<<async_grid[2], 640, async_smem[2], st>>>(a);
+        else if (sign_kernel == 4)
+            k_fused_sign_async<MODE, 768, 192><<<async_grid[3], 768, async_smem[3], st>>>(a);
+        else
+            k_fused_sign<MODE, T><<<sign_grid, T, sign_smem, st>>>(a);
         cudaMemcpyAsync(h_status, q, sizeof(FusedQueue), cudaMemcpyDeviceToHost, st);
     }
 
@@ -315,6 +356,13 @@ struct EngineImpl : EngineBase {
     const uint8_t *g_verify_msgs = nullptr;
 
     // Target of signing attempts in flight; the graph is re-captured on the next batch.
+    int set_sign_kernel(int v) {
+        if (v < 0 || v > kAsyncVariants) return CUDIL_ERR_INVALID;
+        sign_kernel = v;
+        g_sign_key[0] = nullptr;
+        return CUDIL_OK;
+    }
+
     int set_spec_slots(unsigned v) {
         spec_slots = v ? std::min<unsigned>(v, 2u * (unsigned)threads) : (unsigned)threads;
         g_sign_key[0] = nullptr;

@@ -48,7 +48,9 @@ struct Cache {
     static constexpr size_t SL_W1P = SL_W0 + (size_t)K * POLY;
     static constexpr size_t SL_CM = SL_W1P + align256(PM::W1PACKED_BYTES);
     static constexpr size_t SL_SIG = SL_CM + 256;
-    static constexpr size_t SLOT = SL_SIG + align256(PM::SIG_BYTES);
+    // w1 as bytes, thread-major (byte 16 t + m = coefficient t + 16 m), for the hint computation
+    static constexpr size_t SL_W1B = SL_SIG + align256(PM::SIG_BYTES);
+    static constexpr size_t SLOT = SL_W1B + (size_t)K * 256;
     // per-signature slot of the persistent verifier: mu | w1' | c masks | status
     static constexpr size_t VS_MU = 0;
     static constexpr size_t VS_W1 = 64;
@@ -69,6 +71,9 @@ struct FusedQueue {
     unsigned int iters;        // signer block-iterations (summed over blocks)
     unsigned int pad2;
     unsigned long long cyc[4]; // signer cycles per phase summed over blocks: claim, keccak, ntt, total
+    // asynchronous signer, summed over warps: cycles in reject / w / challenge / ExpandMask / claim /
+    // idle polls, then the number of each
+    unsigned long long jobs[12];
 };
 
 // ------------------------------------------------------------------ cache builders
@@ -230,6 +235,7 @@ static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *loc
         q->intt = 0;
         q->iters = 0;
         for (int i = 0; i < 4; ++i) q->cyc[i] = 0;
+        for (int i = 0; i < 12; ++i) q->jobs[i] = 0;
     }
 }
 

@@ -48,6 +48,7 @@ class Engine:
         check(lib.cudil_engine_create(ctypes.byref(h), mode, max_keys, max_items, threads, budget_bytes),
               "cudil_engine_create")
         self.h = h
+        self.set_sign_kernel(t.get("sign_kernel", 0))
         self.set_spec_slots(spec_slots or t["spec_slots"])
 
     def close(self):
@@ -64,6 +65,18 @@ class Engine:
     @property
     def device_bytes(self) -> int:
         return lib.cudil_engine_device_bytes(self.h)
+
+    def set_sign_kernel(self, variant: int):
+        """0 phased persistent signer; 1..4 asynchronous with (threads, slots) per block of
+        (256, 64), (512, 128), (640, 160), (768, 192); see cudil_engine_set_sign_kernel."""
+        check(lib.cudil_engine_set_sign_kernel(self.h, variant), "set_sign_kernel")
+
+    def last_jobs(self) -> dict:
+        """Asynchronous signer job profile of the last batch: {job: (cycles summed over warps, count)}."""
+        v = (ctypes.c_ulonglong * 12)()
+        check(lib.cudil_engine_last_jobs(self.h, v), "last_jobs")
+        names = ("reject", "w", "challenge", "mask", "claim", "idle")
+        return {k: (v[i], v[6 + i]) for i, k in enumerate(names)}
 
     def set_spec_slots(self, slots: int):
         """Per-block target of signing attempts in flight; see cudil_engine_set_spec_slots."""

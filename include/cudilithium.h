@@ -188,6 +188,16 @@ int cudil_engine_last_work(const cudil_engine *e, unsigned long long *attempts, 
  * consecutive nonces in flight (at most 64).  0 = default (threads_per_block).  Takes effect
  * from the next batch. */
 int cudil_engine_set_spec_slots(cudil_engine *e, unsigned spec_slots);
+/* Signer kernel: 0 (default) = phased persistent kernel (block-wide Keccak / NTT phases,
+ * threads_per_block threads); 1..4 = asynchronous persistent kernel -- warps take ready jobs from a
+ * per-block attempt-slot state machine without block barriers, the speculation target capped at
+ * the slot count -- with (threads, slots) per block of (256, 64), (512, 128), (640, 160) and
+ * (768, 192).  Results are identical for every variant. */
+int cudil_engine_set_sign_kernel(cudil_engine *e, int variant);
+/* Job profile of the last batch of the asynchronous signer, summed over warps: SM cycles spent in
+ * rejection / w / challenge / ExpandMask jobs, claims and idle polls (out[0..5]) and their counts
+ * (out[6..11]; challenge and ExpandMask count attempts). */
+int cudil_engine_last_jobs(const cudil_engine *e, unsigned long long out[12]);
 /* Signer phase profile of the last batch: SM cycles summed over blocks spent in slot refills,
  * Keccak phases, NTT phases and in total, and the number of block iterations. */
 int cudil_engine_last_phases(const cudil_engine *e, unsigned long long cycles[4], unsigned *iterations);

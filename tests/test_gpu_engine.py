@@ -124,3 +124,49 @@ def test_engine_argument_errors(cuda_ok, oracle):
     with pytest.raises(CudilError) as ei:
         Engine(5, max_keys=4096, max_items=65536, budget_bytes=1 << 20)
     assert ei.value.code == CUDIL_ERR_BUDGET
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+def test_engine_sign_kernel_variants_match_oracle(cuda_ok, oracle, mode, variant):
+    """Every signer kernel (phased, asynchronous 256/64, asynchronous 512/128) gives the oracle's
+    signatures: many items per block, fewer items than blocks, one item, repeated keys, uneven
+    message lengths, and a batch where several blocks own no item."""
+    import torch
+    from cudilithium_b200.engine import Engine
+    rng = np.random.default_rng(300 + 10 * mode + variant)
+    nk = 5
+    pk, sk = oracle.keypair_batch(mode, nk, rand_index=1300 + mode)
+    eng = Engine(mode, max_keys=nk, max_items=700)
+    eng.set_sign_kernel(variant)
+    eng.set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
+    for n in (700, 97, 1):
+        lens = rng.integers(0, 400, n)
+        msgs = rand_msgs(rng, n, lens)
+        key_idx = rng.integers(0, nk, n).astype(np.uint32)
+        sig = eng.sign_np(msgs, key_idx)
+        want = oracle_sign(oracle, mode, sk, key_idx, msgs)
+        assert np.array_equal(sig, want), f"n={n}"
+        attempts, err = eng.last_status()
+        assert err == 0 and attempts >= n
+    # the accepted signatures verify through the cached public keys
+    eng.set_public_keys(torch.from_numpy(pk.reshape(-1)).cuda())
+    assert np.all(eng.verify_np(sig, msgs, key_idx) == 0)
+
+
+@pytest.mark.parametrize("variant", [1, 3])
+@pytest.mark.parametrize("spec", [1, 8, 0])
+def test_engine_async_speculation_targets(cuda_ok, oracle, variant, spec):
+    """Speculation target 1 (no speculation), 8 and the slot count give the same signatures."""
+    import torch
+    from cudilithium_b200.engine import Engine
+    mode, nk, n = 2, 3, 400
+    rng = np.random.default_rng(77 + spec + variant)
+    pk, sk = oracle.keypair_batch(mode, nk, rand_index=2100)
+    eng = Engine(mode, max_keys=nk, max_items=n)
+    eng.set_sign_kernel(variant)
+    eng.set_spec_slots(spec if spec else 1024)
+    eng.set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
+    msgs = rand_msgs(rng, n, rng.integers(0, 100, n))
+    key_idx = rng.integers(0, nk, n).astype(np.uint32)
+    assert np.array_equal(eng.sign_np(msgs, key_idx), oracle_sign(oracle, mode, sk, key_idx, msgs))
