@@ -49,10 +49,32 @@ OPS_PERM = 24 * 190
 OPS_NTT_FWD = 1024 * 6          # 1024 butterflies: 3 IMAD + 3 IADD
 OPS_NTT_INV = 1024 * 6 + 256 * 4  # + the final multiplication by f
 OPS_PW = 5                        # one Montgomery pointwise product
+# k_fused_sign<2,256>, batch 10000: 1.014292 GB read + 0.488978 GB written per launch (ncu)
+FUSED_SIGN_TRAFFIC_BYTES = 1.014292e9 + 0.488978e9
 
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------- ranks
+# Items are independent, so N GPUs run N replicas over disjoint inputs (no data-path collective).
+def rank_shard(rank: int, batch: int) -> tuple[int, int]:
+    """(key rand_index, message seed) of a rank: keys 2*batch*rank .. of the reference seed scheme
+    (the keypair kernel uses rand_index + 2i + 1, so ranks never share a key) and its own message
+    stream."""
+    return rank * 2 * batch, 1234 + rank
+
+
+def reduce_max(vals, world: int, device):
+    """Element-wise max over ranks of per-rank timings (the job's time is its slowest rank)."""
+    if world == 1:
+        return tuple(vals)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(vals), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return tuple(t.tolist())
 
 
 # ---------------------------------------------------------------------------- clocks
@@ -222,11 +244,7 @@ def run_gpu(args) -> dict | None:
         torch.cuda.synchronize()
 
     def max_over_ranks(*vals):
-        if world == 1:
-            return vals
-        t = torch.tensor(vals, dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return tuple(t.tolist())
+        return reduce_max(vals, world, dev)
 
     # ---- inputs: keys from the reference seed scheme, one key per message
     kp_pool, kpp = alloc_pool(d.keypair_row_bytes(), B)
@@ -236,11 +254,11 @@ def run_gpu(args) -> dict | None:
     for _ in range(2):
         with kg:
             _lib.check(lib.cudil_keypair_dev(mode, d_pk.data_ptr(), d_sk.data_ptr(), None, kp_pool.data_ptr(), kpp,
-                                             B, spp, rank * 2 * B), "keypair")
+                                             B, spp, rank_shard(rank, B)[0]), "keypair")
     torch.cuda.synchronize()
     keygen_ms = kg.pairs[-1][0].elapsed_time(kg.pairs[-1][1])
     del kp_pool
-    rng = np.random.default_rng(1234 + rank)
+    rng = np.random.default_rng(rank_shard(rank, B)[1])
     m_host = rng.integers(0, 256, (B, MLEN), dtype=np.uint8)
     d_m = torch.from_numpy(m_host.reshape(-1)).to(dev)
     keys = np.arange(B, dtype=np.uint32)
@@ -383,7 +401,11 @@ def run_gpu(args) -> dict | None:
     roofline = {
         "bound": "int32-alu", "kernel": "k_fused_sign (persistent, graph with init + prehash)",
         "achieved": achieved, "peak": peak_ops / 1e9, "unit": "Gop/s",
-        "frac": achieved / (peak_ops / 1e9) if achieved else None, "traffic": None,
+        "frac": achieved / (peak_ops / 1e9) if achieved else None,
+        # DRAM bytes per launch of the same signer launch (batch 10000, one key per message) from
+        # one ncu capture: dram__bytes_read.sum + dram__bytes_write.sum
+        "traffic": FUSED_SIGN_TRAFFIC_BYTES if (B == 10000 and mode == 2) else None,
+        "traffic_source": "ncu --set full capture of k_fused_sign<2,256>, bench.py --workload fused-sign --batch 10000",
         "ms_per_launch": g_ms, "launches": 1, "share_of_step": g_ms / total_ms if total_ms else None,
         "attempts": att1, "reject_intt": intt1, "signer_phases": es.last_phases(),
         "ops_model": "Keccak-f1600 = 4560 LOP3/SHF ops; NTT 6144, invNTT 7168, Montgomery product 5",
