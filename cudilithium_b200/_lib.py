@@ -73,6 +73,7 @@ class cudil_serve_stats(ctypes.Structure):
 # Every symbol the public header declares, with its ctypes signature.
 SIGNATURES = {
     "cudil_version": (c_char_p, []),
+    "cudil_last_error": (c_char_p, []),
     "cudil_get_params": (c_int, [c_int, POINTER(cudil_params)]),
     "cudil_keypair_row_bytes": (c_size_t, [c_int]),
     "cudil_sign_row_bytes": (c_size_t, [c_int, c_size_t]),
@@ -147,6 +148,8 @@ lib = _load()
 
 def check(code: int, what: str) -> None:
     if code != CUDIL_OK:
+        if code == CUDIL_ERR_CUDA:
+            what = f"{what} [{lib.cudil_last_error().decode()}]"
         raise CudilError(code, what)
 
 

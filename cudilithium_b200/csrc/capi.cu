@@ -1,5 +1,6 @@
 // extern "C" boundary: run-time parameter-set dispatch onto the per-mode instantiations, pool row
 // size queries, and the NTT microbenchmark kernel.
+#include <cstdio>
 #include <cuda_runtime.h>
 
 #include "../../include/cudilithium.h"
@@ -110,9 +111,23 @@ static void fill_params(cudil_params *o) {
     o->polyeta_packed = PM::POLYETA_PACKED;
 }
 
+namespace cudil {
+static thread_local char g_last_error[256] = "no error";
+
+int cudil_record_cuda_error(cudaError_t e, const char *file, int line) {
+    const char *base = file;
+    for (const char *p = file; *p; ++p)
+        if (*p == '/') base = p + 1;
+    std::snprintf(g_last_error, sizeof g_last_error, "%s (%s:%d)", cudaGetErrorString(e), base, line);
+    return CUDIL_ERR_CUDA;
+}
+}  // namespace cudil
+
 extern "C" {
 
 const char *cudil_version(void) { return "cudilithium_b200 0.1 (Dilithium round 3 v3.1, sm_100a)"; }
+
+const char *cudil_last_error(void) { return cudil::g_last_error; }
 
 int cudil_get_params(int mode, cudil_params *out) {
     if (!out) return CUDIL_ERR_INVALID;

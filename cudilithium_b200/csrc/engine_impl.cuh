@@ -60,8 +60,10 @@ struct EngineImpl : EngineBase {
     using PM = P<MODE>;
     using C = Cache<MODE>;
 
+    // pinned staging: [FusedQueue, padded to 64 bytes | key | mlen | order | off]
+    static constexpr size_t kStageHead = (sizeof(FusedQueue) + 63) / 64 * 64;
     static size_t stage_bytes(size_t max_items) {
-        return 64 + max_items * (3 * sizeof(unsigned) + sizeof(unsigned long long));
+        return kStageHead + max_items * (3 * sizeof(unsigned) + sizeof(unsigned long long));
     }
 
     template <int T>
@@ -90,9 +92,9 @@ struct EngineImpl : EngineBase {
         async_smem[v] = AsyncSignSmem<MODE, T, S>::BYTES;
         if (cudaFuncSetAttribute(k_fused_sign_async<MODE, T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)async_smem[v]) != cudaSuccess)
-            return CUDIL_ERR_CUDA;
+            return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
         async_grid[v] = grid_for<T>((const void *)k_fused_sign_async<MODE, T, S>, async_smem[v], sm_count);
-        return async_grid[v] > 0 ? CUDIL_OK : CUDIL_ERR_CUDA;
+        return async_grid[v] > 0 ? CUDIL_OK : cudil_record_cuda_error(cudaErrorInvalidConfiguration, __FILE__, __LINE__);
     }
 
     int configure_async() {
@@ -109,10 +111,10 @@ struct EngineImpl : EngineBase {
         verify_smem = FusedVerifySmem<MODE, T>::BYTES;
         if (cudaFuncSetAttribute(k_fused_sign<MODE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sign_smem) != cudaSuccess ||
             cudaFuncSetAttribute(k_fused_verify<MODE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)verify_smem) != cudaSuccess)
-            return CUDIL_ERR_CUDA;
+            return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
         sign_grid = grid_for<T>((const void *)k_fused_sign<MODE, T>, sign_smem, sm_count);
         verify_grid = grid_for<T>((const void *)k_fused_verify<MODE, T>, verify_smem, sm_count);
-        return (sign_grid > 0 && verify_grid > 0) ? CUDIL_OK : CUDIL_ERR_CUDA;
+        return (sign_grid > 0 && verify_grid > 0) ? CUDIL_OK : cudil_record_cuda_error(cudaErrorInvalidConfiguration, __FILE__, __LINE__);
     }
 
     int create(size_t mk, size_t mi, int thr, size_t budget) {
@@ -122,8 +124,8 @@ struct EngineImpl : EngineBase {
         threads = thr;
         // mk == 0: caches attached later; mi == 0: a cache-only engine other engines attach to
         if ((mi == 0 && mk == 0) || mi > (1u << 24)) return CUDIL_ERR_INVALID;
-        if (cudaGetDevice(&device) != cudaSuccess) return CUDIL_ERR_CUDA;
-        if (cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return CUDIL_ERR_CUDA;
+        CUDIL_CK(cudaGetDevice(&device));
+        CUDIL_CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
         int rc = (threads == 128) ? configure<128>() : (threads == 256 ? configure<256>() : CUDIL_ERR_INVALID);
         if (rc) return rc;
         rc = configure_async();
@@ -147,9 +149,10 @@ struct EngineImpl : EngineBase {
                     cudaMalloc(&scratch, scratch_bytes) != cudaSuccess)) ||
             cudaMalloc(&q, sizeof(FusedQueue)) != cudaSuccess || cudaMallocHost(&h_stage, stage_bytes(mi)) != cudaSuccess ||
             cudaMallocHost(&h_status, sizeof(FusedQueue)) != cudaSuccess)
-            return CUDIL_ERR_CUDA;
+            return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
         std::memset(h_status, 0, sizeof(FusedQueue));
-        return cudaMemset(q, 0, sizeof(FusedQueue)) == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
+        CUDIL_CK(cudaMemset(q, 0, sizeof(FusedQueue)));
+        return CUDIL_OK;
     }
 
     ~EngineImpl() override {
@@ -225,11 +228,11 @@ struct EngineImpl : EngineBase {
     int upload_meta(const unsigned long long *off, const unsigned *mlen, const unsigned *key, size_t n, size_t nkeys,
                     size_t msgs_bytes, bool longest_first, cudaStream_t st) {
         // the previous batch's upload from the staging buffer must have completed
-        if (cudaStreamSynchronize(st) != cudaSuccess) return CUDIL_ERR_CUDA;
+        CUDIL_CK(cudaStreamSynchronize(st));
         FusedQueue *hq = reinterpret_cast<FusedQueue *>(h_stage);
         std::memset(hq, 0, sizeof(FusedQueue));
         hq->n = (unsigned)n;
-        unsigned *hk = reinterpret_cast<unsigned *>(h_stage + 64);
+        unsigned *hk = reinterpret_cast<unsigned *>(h_stage + kStageHead);
         unsigned *hm = hk + max_items;
         unsigned *ho = hm + max_items;
         unsigned long long *hoff = reinterpret_cast<unsigned long long *>(ho + max_items);
@@ -297,11 +300,11 @@ struct EngineImpl : EngineBase {
         }
         cudaStreamDestroy(cs);
         (void)st;
-        if (e != cudaSuccess) return CUDIL_ERR_CUDA;
+        if (e != cudaSuccess) return cudil_record_cuda_error(e, __FILE__, __LINE__);
         if (*exec) cudaGraphExecDestroy(*exec);
         e = cudaGraphInstantiate(exec, graph, 0);
         cudaGraphDestroy(graph);
-        return e == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
+        return e == cudaSuccess ? CUDIL_OK : cudil_record_cuda_error(e, __FILE__, __LINE__);
     }
 
     int sign(uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes, const unsigned long long *off, const unsigned *mlen,

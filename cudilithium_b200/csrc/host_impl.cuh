@@ -18,16 +18,20 @@
 
 namespace cudil {
 
-#define CUDIL_CK(x)                                       \
-    do {                                                  \
-        if ((x) != cudaSuccess) return CUDIL_ERR_CUDA;    \
+// Records the failing CUDA call of this host thread (cudil_last_error) and returns its status.
+int cudil_record_cuda_error(cudaError_t e, const char *file, int line);
+#define CUDIL_CK(x)                                                         \
+    do {                                                                    \
+        const cudaError_t cudil_e_ = (x);                                   \
+        if (cudil_e_ != cudaSuccess) return ::cudil::cudil_record_cuda_error(cudil_e_, __FILE__, __LINE__); \
     } while (0)
-#define CUDIL_CK_LAUNCH()                                       \
-    do {                                                        \
-        if (cudaPeekAtLastError() != cudaSuccess) {             \
-            (void)cudaGetLastError();                           \
-            return CUDIL_ERR_CUDA;                              \
-        }                                                       \
+#define CUDIL_CK_LAUNCH()                                                   \
+    do {                                                                    \
+        const cudaError_t cudil_e_ = cudaPeekAtLastError();                 \
+        if (cudil_e_ != cudaSuccess) {                                      \
+            (void)cudaGetLastError();                                       \
+            return ::cudil::cudil_record_cuda_error(cudil_e_, __FILE__, __LINE__);   \
+        }                                                                   \
     } while (0)
 
 // Pools are addressed with 8- and 16-byte vector accesses: base and pitch must be 16-byte aligned

@@ -26,6 +26,15 @@
 
 #include "../../include/cudilithium.h"
 
+namespace cudil {
+int cudil_record_cuda_error(cudaError_t e, const char *file, int line);
+}
+#define SRV_CK(x)                                                                              \
+    do {                                                                                       \
+        const cudaError_t srv_e_ = (x);                                                        \
+        if (srv_e_ != cudaSuccess) return ::cudil::cudil_record_cuda_error(srv_e_, __FILE__, __LINE__); \
+    } while (0)
+
 namespace {
 
 using Clock = std::chrono::steady_clock;
@@ -114,8 +123,8 @@ struct Slot {
         }
         const size_t msg_bytes = (cfg->path == 0) ? std::max<size_t>(pos, 8) : n * cfg->max_mlen;
         const auto c1 = Clock::now();
-        if (cudaMemcpyAsync(d_msgs, h_msgs, msg_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) return CUDIL_ERR_CUDA;
-        if (op == 1 && cudaMemcpyAsync(d_sig, h_sig, n * sigb, cudaMemcpyHostToDevice, st) != cudaSuccess) return CUDIL_ERR_CUDA;
+        SRV_CK(cudaMemcpyAsync(d_msgs, h_msgs, msg_bytes, cudaMemcpyHostToDevice, st));
+        if (op == 1) SRV_CK(cudaMemcpyAsync(d_sig, h_sig, n * sigb, cudaMemcpyHostToDevice, st));
         int rc = CUDIL_OK;
         const int mi = mode_index(mode);
         if (cfg->path == 0) {
@@ -130,7 +139,7 @@ struct Slot {
             for (size_t i = 0; i < n; ++i) std::memcpy(h_keys + i * kb, src + (size_t)key[i] * kb, kb);
             if (cudaMemcpyAsync(d_keys, h_keys, n * kb, cudaMemcpyHostToDevice, st) != cudaSuccess ||
                 cudaMemcpyAsync(d_mlens, h_mlens, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st) != cudaSuccess)
-                return CUDIL_ERR_CUDA;
+                return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
             if (op == 0) {
                 sign_lut.assign(n, cudil_sign_lut_element{0, 0});
                 lut.sign_lut = sign_lut.data();
@@ -144,11 +153,11 @@ struct Slot {
         }
         if (rc) return rc;
         if (op == 0) {
-            if (cudaMemcpyAsync(h_sig, d_sig, n * sigb, cudaMemcpyDeviceToHost, st) != cudaSuccess) return CUDIL_ERR_CUDA;
+            SRV_CK(cudaMemcpyAsync(h_sig, d_sig, n * sigb, cudaMemcpyDeviceToHost, st));
         } else {
-            if (cudaMemcpyAsync(h_ret, d_ret, n * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return CUDIL_ERR_CUDA;
+            SRV_CK(cudaMemcpyAsync(h_ret, d_ret, n * sizeof(int), cudaMemcpyDeviceToHost, st));
         }
-        if (cudaStreamSynchronize(st) != cudaSuccess) return CUDIL_ERR_CUDA;
+        SRV_CK(cudaStreamSynchronize(st));
         const auto c2 = Clock::now();
         if (cfg->path == 0 && op == 0) {
             unsigned long long att = 0;
@@ -259,18 +268,18 @@ int make_slot(Slot &s, const cudil_serve_config *cfg, Trace *tr, cudil_engine *c
         if (rc) return rc;
         if (cfg->engine_spec_slots) cudil_engine_set_spec_slots(s.eng, (unsigned)cfg->engine_spec_slots);
     }
-    if (cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking) != cudaSuccess) return CUDIL_ERR_CUDA;
+    SRV_CK(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
     s.msgs_cap = (cfg->path == 0) ? B * al8(cfg->max_mlen) + 8 : B * (size_t)cfg->max_mlen + 8;
     if (cudaMalloc(&s.d_msgs, s.msgs_cap) != cudaSuccess || cudaMalloc(&s.d_sig, B * p.sig_bytes) != cudaSuccess ||
         cudaMalloc(&s.d_ret, B * sizeof(int)) != cudaSuccess || cudaMallocHost(&s.h_msgs, s.msgs_cap) != cudaSuccess ||
         cudaMallocHost(&s.h_sig, B * p.sig_bytes) != cudaSuccess || cudaMallocHost(&s.h_ret, B * sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&s.h_mlens, B * sizeof(uint32_t)) != cudaSuccess)
-        return CUDIL_ERR_CUDA;
+        return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
     if (cfg->path == 1) {
         const size_t kb = (s.op == 0) ? (size_t)p.sk_bytes : (size_t)p.pk_bytes;
         if (cudaMalloc(&s.d_keys, B * kb) != cudaSuccess || cudaMalloc(&s.d_mlens, B * sizeof(uint32_t)) != cudaSuccess ||
             cudaMallocHost(&s.h_keys, B * kb) != cudaSuccess)
-            return CUDIL_ERR_CUDA;
+            return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
         if (s.op == 0) {
             const size_t T = (size_t)cfg->plain_exec_threshold;
             s.pitch = pitch512(cudil_sign_row_bytes(s.mode, cfg->max_mlen));
@@ -280,10 +289,10 @@ int make_slot(Slot &s, const cudil_serve_config *cfg, Trace *tr, cudil_engine *c
                 cudaMalloc(&s.lut.d_copy_lut, T * sizeof(cudil_copy_lut_element)) != cudaSuccess ||
                 cudaMallocHost(&s.lut.h_exec_lut, T * 4) != cudaSuccess || cudaMallocHost(&s.lut.h_done_lut, T) != cudaSuccess ||
                 cudaMallocHost(&s.lut.h_copy_lut, T * sizeof(cudil_copy_lut_element)) != cudaSuccess)
-                return CUDIL_ERR_CUDA;
+                return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
         } else {
             s.pitch = pitch512(cudil_verify_row_bytes(s.mode, cfg->max_mlen));
-            if (cudaMalloc(&s.pool, B * s.pitch) != cudaSuccess) return CUDIL_ERR_CUDA;
+            SRV_CK(cudaMalloc(&s.pool, B * s.pitch));
         }
     }
     s.device_bytes = own + (s.eng ? cudil_engine_device_bytes(s.eng) : 0);
@@ -324,7 +333,7 @@ extern "C" int cudil_serve_trace(const cudil_serve_config *cfg, const uint8_t *c
         used[mi] = true;
     }
     int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess) return CUDIL_ERR_CUDA;
+    SRV_CK(cudaGetDevice(&device));
 
     // resident key caches (fused path): one cache engine per parameter set
     cudil_engine *cache[3] = {nullptr, nullptr, nullptr};
@@ -357,7 +366,7 @@ extern "C" int cudil_serve_trace(const cudil_serve_config *cfg, const uint8_t *c
             uint8_t *d = nullptr;
             const size_t kbytes = tr.nkeys[m] * (size_t)std::max(p.sk_bytes, p.pk_bytes);
             if (cudaMalloc(&d, kbytes) != cudaSuccess) {
-                rc = CUDIL_ERR_CUDA;
+                rc = ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
                 break;
             }
             if (tr.sk[m]) {

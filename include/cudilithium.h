@@ -65,6 +65,9 @@ typedef struct {
 
 /* Library / parameter queries. */
 const char *cudil_version(void);
+/* Text of the last CUDA failure reported as CUDIL_ERR_CUDA on the calling host thread (the CUDA
+ * error string and the library source location), "no error" before any. */
+const char *cudil_last_error(void);
 int cudil_get_params(int mode, cudil_params *out);
 
 /* Minimum per-item row sizes of the caller-allocated pitched pools.  They equal the reference's

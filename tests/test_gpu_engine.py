@@ -170,3 +170,19 @@ def test_engine_async_speculation_targets(cuda_ok, oracle, variant, spec):
     msgs = rand_msgs(rng, n, rng.integers(0, 100, n))
     key_idx = rng.integers(0, nk, n).astype(np.uint32)
     assert np.array_equal(eng.sign_np(msgs, key_idx), oracle_sign(oracle, mode, sk, key_idx, msgs))
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_engine_single_item_capacity(cuda_ok, oracle, mode):
+    """An engine sized for one item (smallest staging buffers) signs and verifies correctly."""
+    import torch
+    from cudilithium_b200.engine import Engine
+    pk, sk = oracle.keypair_batch(mode, 2, rand_index=3100 + mode)
+    eng = Engine(mode, max_keys=2, max_items=1)
+    eng.set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
+    eng.set_public_keys(torch.from_numpy(pk.reshape(-1)).cuda())
+    msg = [b"single item capacity"]
+    sig = eng.sign_np(msg, np.array([1], np.uint32))
+    assert np.array_equal(sig, oracle_sign(oracle, mode, sk, [1], msg))
+    assert eng.verify_np(sig, msg, np.array([1], np.uint32))[0] == 0
+    assert eng.verify_np(sig, msg, np.array([0], np.uint32))[0] == -1
