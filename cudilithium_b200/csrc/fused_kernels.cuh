@@ -366,7 +366,9 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
             base = __shfl_sync(0xFFFFFFFFu, base, 0);
             if ((int)base >= total) break;
             const int job = (int)base + lane;
-            if (job < na_c) {
+            // attempts above an already accepted nonce of their item are skipped (they cannot win)
+            if (job < na_c && __ldcg(arg.best + s_item[cb * A + job]) < s_nonce[cb * A + job]) {
+            } else if (job < na_c) {
                 const unsigned item = s_item[cb * A + job];
                 uint8_t *slot = slot_of(cb, job);
                 uint32_t al[25], ah[25];
@@ -385,6 +387,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                 for (int k = 0; k < 4; ++k)
                     mo[k] = make_uint4(mask[(4 * k) * THREADS], mask[(4 * k + 1) * THREADS], mask[(4 * k + 2) * THREADS],
                                        mask[(4 * k + 3) * THREADS]);
+            } else if (job < total && __ldcg(arg.best + s_item[nb * A + (job - na_c) / L]) < s_nonce[nb * A + (job - na_c) / L]) {
             } else if (job < total) {
                 const int idx = job - na_c, a = idx / L, j = idx % L;
                 const unsigned item = s_item[nb * A + a], nonce = s_nonce[nb * A + a];
@@ -400,7 +403,10 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
     // rejection checks, hints and publication of one attempt (group-collective)
     auto reject_job = [&](int cb, int a) {
         const unsigned item = s_item[cb * A + a], nonce = s_nonce[cb * A + a];
-        if (nonce > 0xFFFFu) {
+        // one decision per group: out-of-range nonce, or a smaller nonce of the item already accepted
+        bool skip = nonce > 0xFFFFu || __ldcg(arg.best + item) < nonce;
+        skip = __shfl_sync(g.gmask, skip, lane_off);
+        if (skip) {
             if (g.t == 0) atomicSub(arg.inflight + item, 1u);
             return;
         }
@@ -570,6 +576,9 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
     // w = invNTT(A_hat * NTT(y)), Decompose, pack w1 of one attempt (group-collective)
     auto w_job = [&](int nb, int a) {
         const unsigned item = s_item[nb * A + a];
+        bool skip = __ldcg(arg.best + item) < s_nonce[nb * A + a];
+        skip = __shfl_sync(g.gmask, skip, lane_off);
+        if (skip) return;
         uint8_t *slot = slot_of(nb, a);
         const uint8_t *row = arg.cache + (size_t)arg.key_idx[item] * arg.cpitch;
         int32_t *yh = reinterpret_cast<int32_t *>(ph) + (size_t)gi * (L * N + NTT_SMEM_WORDS);

@@ -64,13 +64,13 @@ struct Impl {
         const int nn = (int)n;
         CUDIL_CK(cudaMemset2DAsync(pool + LY::KP_TACC, pitch, 0, (size_t)K * LY::POLY, n, st));
         if (seeds) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::KP_SK + PM::SK_TR, pitch, seeds, SEEDBYTES, SEEDBYTES, n, in_kind, st));
-        CUDIL_LAUNCH(KID_KP_SEED, st, k_kp_seed<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, nn, (unsigned long long)rand_index, seeds ? 1 : 0));
+        CUDIL_LAUNCH(KID_KP_SEED, st, k_kp_seed<MODE><<<blocks_for(n, kItemBlock), kItemBlock, 0, st>>>(pool, pitch, nn, (unsigned long long)rand_index, seeds ? 1 : 0));
         CUDIL_CK_LAUNCH();
         const size_t smem = KpSmem<MODE>::bytes(KPI);
         CUDIL_CK(cudaFuncSetAttribute(k_kp_main<MODE, KPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         CUDIL_LAUNCH(KID_KP_MAIN, st, k_kp_main<MODE, KPI><<<(unsigned)((n + KPI - 1) / KPI), kBlock, smem, st>>>(pool, pitch, nn));
         CUDIL_CK_LAUNCH();
-        CUDIL_LAUNCH(KID_KP_TR, st, k_kp_tr<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, nn));
+        CUDIL_LAUNCH(KID_KP_TR, st, k_kp_tr<MODE><<<blocks_for(n, kItemBlock), kItemBlock, 0, st>>>(pool, pitch, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_CK(cudaMemcpy2DAsync(pk, PM::PK_BYTES, pool + LY::KP_PK, pitch, PM::PK_BYTES, n, out_kind, st));
         CUDIL_CK(cudaMemcpy2DAsync(sk, PM::SK_BYTES, pool + LY::KP_SK, pitch, PM::SK_BYTES, n, out_kind, st));
@@ -83,7 +83,7 @@ struct Impl {
         const int nn = (int)n;
         if (mlen) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::SG_MSG, sp, m, m_pitch, mlen, n, in_kind, st));
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::SG_SK, sp, sk, sk_pitch, PM::SK_BYTES, n, in_kind, st));
-        CUDIL_LAUNCH(KID_SIGN_PREHASH, st, k_sign_prehash<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, sp, mlen, mlens, nn));
+        CUDIL_LAUNCH(KID_SIGN_PREHASH, st, k_sign_prehash<MODE><<<blocks_for(n, kItemBlock), kItemBlock, 0, st>>>(pool, sp, mlen, mlens, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_EXPAND_A, st, k_expand_a<MODE><<<blocks_for(n * K * L), kBlock, 0, st>>>(pool, sp, LY::SG_SK + PM::SK_RHO, LY::sg_mat(mlen), nn));
         CUDIL_CK_LAUNCH();
@@ -99,7 +99,7 @@ struct Impl {
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_SIGN_COMPUTE_W, st, k_sign_compute_w<MODE, AW><<<(unsigned)((nexec + AW - 1) / AW), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, nexec));
         CUDIL_CK_LAUNCH();
-        CUDIL_LAUNCH(KID_SIGN_CHALLENGE, st, k_sign_challenge<MODE><<<blocks_for((size_t)nexec), kBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec));
+        CUDIL_LAUNCH(KID_SIGN_CHALLENGE, st, k_sign_challenge<MODE><<<blocks_for((size_t)nexec, kItemBlock), kItemBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_SIGN_REJECT, st, k_sign_reject<MODE><<<blocks_for((size_t)nexec * 16), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, d_done, nexec));
         CUDIL_CK_LAUNCH();
@@ -199,13 +199,13 @@ struct Impl {
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::VF_SIG, pitch, sig, sig_pitch, PM::SIG_BYTES, n, in_kind, st));
         if (mlen) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::VF_TRM + SEEDBYTES, pitch, m, m_pitch, mlen, n, in_kind, st));
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::VF_PK, pitch, pk, pk_pitch, PM::PK_BYTES, n, in_kind, st));
-        CUDIL_LAUNCH(KID_VERIFY_PREPARE, st, k_verify_prepare<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, mlen, mlens, nn));
+        CUDIL_LAUNCH(KID_VERIFY_PREPARE, st, k_verify_prepare<MODE><<<blocks_for(n, kItemBlock), kItemBlock, 0, st>>>(pool, pitch, mlen, mlens, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_EXPAND_A, st, k_expand_a<MODE><<<blocks_for(n * K * L), kBlock, 0, st>>>(pool, pitch, LY::VF_PK, LY::vf_mat(mlen), nn));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_VERIFY_W, st, k_verify_w<MODE, AV><<<(unsigned)((n + AV - 1) / AV), kBlock, 0, st>>>(pool, pitch, mlen, nn));
         CUDIL_CK_LAUNCH();
-        CUDIL_LAUNCH(KID_VERIFY_FINAL, st, k_verify_final<MODE><<<blocks_for(n), kBlock, 0, st>>>(pool, pitch, mlen, nn));
+        CUDIL_LAUNCH(KID_VERIFY_FINAL, st, k_verify_final<MODE><<<blocks_for(n, kItemBlock), kItemBlock, 0, st>>>(pool, pitch, mlen, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_CK(cudaMemcpy2DAsync(ret, sizeof(int), pool + LY::vf_aux(mlen) + 68, pitch, sizeof(int), n, out_kind, st));
         return CUDIL_OK;

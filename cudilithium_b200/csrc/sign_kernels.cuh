@@ -19,6 +19,7 @@ namespace cudil {
 
 constexpr int kBlock = 128;             // threads per block for the SHAKE-stream kernels
 constexpr int kGroupsPerBlock = 8;      // 16-thread groups per 128-thread block
+constexpr int kItemBlock = 32;          // threads per block for thread-per-item kernels
 
 // ------------------------------------------------------------------ per-item setup
 
@@ -241,13 +242,15 @@ __device__ __forceinline__ void sample_in_ball(const uint2 (&ct)[4], uint32_t *b
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_sign_challenge(const uint8_t *sign_pool, size_t sp, uint8_t *temp_pool, size_t tp,
-                                                           const uint32_t *exec_lut, int nexec) {
+// Thread-per-item kernels run TB = kItemBlock threads per block so that batches of a few thousand
+// items still spread over every SM.
+template <int MODE, int TB = kItemBlock>
+__global__ void __launch_bounds__(TB) k_sign_challenge(const uint8_t *sign_pool, size_t sp, uint8_t *temp_pool, size_t tp,
+                                                       const uint32_t *exec_lut, int nexec) {
     using PM = P<MODE>;
     using LY = Layout<MODE>;
-    __shared__ uint32_t s_blk[2 * 17][kBlock];
-    __shared__ uint32_t s_mask[16][kBlock];
+    __shared__ uint32_t s_blk[2 * 17][TB];
+    __shared__ uint32_t s_mask[16][TB];
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nexec) return;
     const uint32_t item = exec_lut[e] >> 16;
@@ -263,11 +266,11 @@ __global__ void __launch_bounds__(kBlock) k_sign_challenge(const uint8_t *sign_p
 #pragma unroll
     for (int w = 0; w < 4; ++w) sig_ct[w] = ct[w];
     uint32_t *mask = &s_mask[0][threadIdx.x];
-    sample_in_ball<PM::TAU, kBlock>(ct, &s_blk[0][threadIdx.x], mask);
+    sample_in_ball<PM::TAU, TB>(ct, &s_blk[0][threadIdx.x], mask);
     uint4 *mo = reinterpret_cast<uint4 *>(trow + LY::TP_CMASK);
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-        mo[k] = make_uint4(mask[(4 * k) * kBlock], mask[(4 * k + 1) * kBlock], mask[(4 * k + 2) * kBlock], mask[(4 * k + 3) * kBlock]);
+        mo[k] = make_uint4(mask[(4 * k) * TB], mask[(4 * k + 1) * TB], mask[(4 * k + 2) * TB], mask[(4 * k + 3) * TB]);
 }
 
 // One group per attempt: c_hat = NTT(c); z = y + c*s1 (norm check, pack); r0 = w0 - c*s2 and c*t0

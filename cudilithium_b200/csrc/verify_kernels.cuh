@@ -12,14 +12,14 @@
 
 namespace cudil {
 
-template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_verify_prepare(uint8_t *pool, size_t pitch, size_t mlen, const uint32_t *mlens,
-                                                           int n) {
+template <int MODE, int TB = kItemBlock>
+__global__ void __launch_bounds__(TB) k_verify_prepare(uint8_t *pool, size_t pitch, size_t mlen, const uint32_t *mlens,
+                                                       int n) {
     using PM = P<MODE>;
     using LY = Layout<MODE>;
     constexpr int K = PM::K, OMEGA = PM::OMEGA;
-    __shared__ uint32_t s_blk[2 * 17][kBlock];
-    __shared__ uint32_t s_mask[16][kBlock];
+    __shared__ uint32_t s_blk[2 * 17][TB];
+    __shared__ uint32_t s_mask[16][TB];
     const int it = blockIdx.x * blockDim.x + threadIdx.x;
     if (it >= n) return;
     uint8_t *row = pool + (size_t)it * pitch;
@@ -66,11 +66,11 @@ __global__ void __launch_bounds__(kBlock) k_verify_prepare(uint8_t *pool, size_t
     uint2 ct[4];
     ld_lanes(ct, row + LY::VF_SIG);
     uint32_t *mask = &s_mask[0][threadIdx.x];
-    sample_in_ball<PM::TAU, kBlock>(ct, &s_blk[0][threadIdx.x], mask);
+    sample_in_ball<PM::TAU, TB>(ct, &s_blk[0][threadIdx.x], mask);
     uint4 *mo = reinterpret_cast<uint4 *>(aux);
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-        mo[k] = make_uint4(mask[(4 * k) * kBlock], mask[(4 * k + 1) * kBlock], mask[(4 * k + 2) * kBlock], mask[(4 * k + 3) * kBlock]);
+        mo[k] = make_uint4(mask[(4 * k) * TB], mask[(4 * k + 1) * TB], mask[(4 * k + 2) * TB], mask[(4 * k + 3) * TB]);
     reinterpret_cast<int *>(aux + 64)[0] = status;
 }
 
