@@ -85,6 +85,12 @@ SIGNATURES = {
     "cudil_sign": (c_int, [c_int, c_void_p, c_size_t, POINTER(c_size_t), c_void_p, c_size_t, c_size_t, c_void_p,
                            c_void_p, c_size_t, c_void_p, c_size_t, POINTER(cudil_task_lut), c_size_t, c_size_t,
                            c_void_p]),
+    "cudil_sign_randomized": (c_int, [c_int, c_void_p, c_size_t, POINTER(c_size_t), c_void_p, c_size_t, c_size_t,
+                                      c_void_p, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p, c_size_t,
+                                      POINTER(cudil_task_lut), c_size_t, c_size_t, c_void_p]),
+    "cudil_sign_dev_randomized": (c_int, [c_int, c_void_p, c_size_t, c_void_p, c_size_t, c_size_t, c_void_p, c_void_p,
+                                          c_size_t, c_void_p, c_size_t, c_void_p, c_size_t, POINTER(cudil_task_lut),
+                                          c_size_t, c_size_t, c_void_p]),
     "cudil_sign_dev": (c_int, [c_int, c_void_p, c_size_t, c_void_p, c_size_t, c_size_t, c_void_p, c_void_p, c_size_t,
                                c_void_p, c_size_t, POINTER(cudil_task_lut), c_size_t, c_size_t, c_void_p]),
     "cudil_verify": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t, c_void_p,
@@ -108,6 +114,8 @@ SIGNATURES = {
     "cudil_engine_set_public_keys": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
     "cudil_engine_sign": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_size_t,
                                   c_void_p]),
+    "cudil_engine_sign_randomized": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p,
+                                             c_void_p, c_size_t, c_void_p]),
     "cudil_engine_verify": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p,
                                     c_size_t, c_void_p]),
     "cudil_engine_last_status": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong), POINTER(c_uint32)]),

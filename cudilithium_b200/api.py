@@ -154,7 +154,10 @@ class Dilithium:
         return (pk.numpy()[: n * self.CRYPTO_PUBLICKEYBYTES].reshape(n, self.CRYPTO_PUBLICKEYBYTES).copy(),
                 sk.numpy()[: n * self.CRYPTO_SECRETKEYBYTES].reshape(n, self.CRYPTO_SECRETKEYBYTES).copy())
 
-    def sign(self, m: np.ndarray, sk: np.ndarray, exec_threshold: int = 2048, return_lut: bool = False):
+    def sign(self, m: np.ndarray, sk: np.ndarray, exec_threshold: int = 2048, return_lut: bool = False,
+             rhoprime: np.ndarray | None = None):
+        """rhoprime: optional (n, 64) random seeds for randomized signing (cudil_sign_randomized);
+        None = deterministic signing."""
         m = np.ascontiguousarray(m, dtype=np.uint8)
         n, mlen = m.shape
         pool, sp = alloc_pool(self.sign_row_bytes(mlen), n)
@@ -166,8 +169,16 @@ class Dilithium:
         hsk.numpy()[: n * self.CRYPTO_SECRETKEYBYTES] = np.ascontiguousarray(sk, dtype=np.uint8).reshape(-1)
         hsig = pinned(n * self.CRYPTO_BYTES)
         siglen = [0]
-        self.crypto_sign_signature(hsig, self.CRYPTO_BYTES, siglen, hm, mlen, mlen, hsk, pool, sp, tpool, tp, lut,
-                                   exec_threshold, n)
+        if rhoprime is None:
+            self.crypto_sign_signature(hsig, self.CRYPTO_BYTES, siglen, hm, mlen, mlen, hsk, pool, sp, tpool, tp, lut,
+                                       exec_threshold, n)
+        else:
+            hr = pinned(n * 64)
+            hr.numpy()[: n * 64] = np.ascontiguousarray(rhoprime, dtype=np.uint8).reshape(-1)
+            sl = ctypes.c_size_t(0)
+            check(lib.cudil_sign_randomized(self.mode, _ptr(hsig), self.CRYPTO_BYTES, ctypes.byref(sl), _ptr(hm), mlen,
+                                            mlen, _ptr(hsk), _ptr(hr), 64, _ptr(pool), sp, _ptr(tpool), tp,
+                                            ctypes.byref(lut.c), exec_threshold, n, None), "cudil_sign_randomized")
         torch.cuda.synchronize()
         sig = hsig.numpy()[: n * self.CRYPTO_BYTES].reshape(n, self.CRYPTO_BYTES).copy()
         return (sig, lut) if return_lut else sig

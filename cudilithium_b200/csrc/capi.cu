@@ -171,6 +171,27 @@ int cudil_sign(int mode, uint8_t *sig, size_t sig_pitch, size_t *siglen, const u
                                  cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost))
 }
 
+int cudil_sign_randomized(int mode, uint8_t *sig, size_t sig_pitch, size_t *siglen, const uint8_t *m, size_t m_pitch,
+                          size_t mlen, const uint8_t *sk, const uint8_t *rhoprime, size_t rhoprime_pitch,
+                          uint8_t *d_sign_pool, size_t sign_pitch, uint8_t *d_temp_pool, size_t temp_pitch,
+                          cudil_task_lut *lut, size_t exec_threshold, size_t batch, void *stream) {
+    if (!rhoprime && batch) return CUDIL_ERR_INVALID;
+    CUDIL_DISPATCH(mode, I::sign(sig, sig_pitch, siglen, m, m_pitch, mlen, sk, I::PM::SK_BYTES, d_sign_pool, sign_pitch,
+                                 d_temp_pool, temp_pitch, lut, exec_threshold, batch, (cudaStream_t)stream,
+                                 cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, nullptr, rhoprime, rhoprime_pitch))
+}
+
+int cudil_sign_dev_randomized(int mode, uint8_t *d_sig, size_t sig_pitch, const uint8_t *d_m, size_t m_pitch,
+                              size_t mlen, const uint8_t *d_sk, const uint8_t *d_rhoprime, size_t rhoprime_pitch,
+                              uint8_t *d_sign_pool, size_t sign_pitch, uint8_t *d_temp_pool, size_t temp_pitch,
+                              cudil_task_lut *lut, size_t exec_threshold, size_t batch, void *stream) {
+    if (!d_rhoprime && batch) return CUDIL_ERR_INVALID;
+    CUDIL_DISPATCH(mode, I::sign(d_sig, sig_pitch, nullptr, d_m, m_pitch, mlen, d_sk, I::PM::SK_BYTES, d_sign_pool,
+                                 sign_pitch, d_temp_pool, temp_pitch, lut, exec_threshold, batch, (cudaStream_t)stream,
+                                 cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice, nullptr, d_rhoprime,
+                                 rhoprime_pitch))
+}
+
 int cudil_sign_dev(int mode, uint8_t *d_sig, size_t sig_pitch, const uint8_t *d_m, size_t m_pitch, size_t mlen,
                    const uint8_t *d_sk, uint8_t *d_sign_pool, size_t sign_pitch, uint8_t *d_temp_pool, size_t temp_pitch,
                    cudil_task_lut *lut, size_t exec_threshold, size_t batch, void *stream) {

@@ -95,6 +95,13 @@ int cudil_engine_sign(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, si
     CUDIL_ENGINE_DISPATCH(e, sign(d_sig, d_msgs, msgs_bytes, offsets, mlens, key_idx, n, (cudaStream_t)stream));
 }
 
+int cudil_engine_sign_randomized(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
+                                 const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx,
+                                 const uint8_t *d_rhoprime, size_t n, void *stream) {
+    if (!d_rhoprime && n) return CUDIL_ERR_INVALID;
+    CUDIL_ENGINE_DISPATCH(e, sign(d_sig, d_msgs, msgs_bytes, offsets, mlens, key_idx, n, (cudaStream_t)stream, d_rhoprime));
+}
+
 int cudil_engine_verify(cudil_engine *e, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
                         const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
                         void *stream) {

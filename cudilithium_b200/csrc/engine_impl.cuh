@@ -48,7 +48,7 @@ struct EngineBase {
     size_t async_smem[kAsyncVariants] = {0, 0, 0, 0};
     // instantiated graphs, keyed by the output / message buffers they were captured with
     cudaGraphExec_t g_sign = nullptr, g_verify = nullptr;
-    const void *g_sign_key[2] = {nullptr, nullptr}, *g_verify_key[2] = {nullptr, nullptr};
+    const void *g_sign_key[3] = {nullptr, nullptr, nullptr}, *g_verify_key[2] = {nullptr, nullptr};
     cudaStream_t g_sign_stream = nullptr, g_verify_stream = nullptr;
     size_t device_bytes = 0;
     bool owns_cache = true;  // false when the key caches belong to another engine (attach_keys)
@@ -256,8 +256,8 @@ struct EngineImpl : EngineBase {
 
     // ------------------------------------------------------------ graphs
     template <int T>
-    void record_sign(cudaStream_t st, uint8_t *d_sig, const uint8_t *d_msgs) {
-        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order};
+    void record_sign(cudaStream_t st, uint8_t *d_sig, const uint8_t *d_msgs, const uint8_t *d_rhop) {
+        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order, d_rhop};
         k_fused_init<<<std::max(1, sm_count * 2), 256, 0, st>>>(q, best, locks, next_nonce, inflight);
         k_fused_prehash<MODE><<<prehash_grid, kBlock, 0, st>>>(sk_cache, sk_pitch, mr, items, q);
         FusedSignArgs a{sk_cache, sk_pitch, d_key, items, d_sig, (size_t)PM::SIG_BYTES, scratch, q, best, locks, next_nonce,
@@ -277,7 +277,7 @@ struct EngineImpl : EngineBase {
 
     template <int T>
     void record_verify(cudaStream_t st, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs) {
-        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order};
+        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order, nullptr};
         k_fused_init<<<1, 32, 0, st>>>(q, best, locks, nullptr, nullptr);
         k_fused_verify<MODE, T><<<verify_grid, T, verify_smem, st>>>(pk_cache, pk_pitch, mr, d_sig, PM::SIG_BYTES, d_ret,
                                                                     scratch, q);
@@ -292,7 +292,7 @@ struct EngineImpl : EngineBase {
         cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             if (sign)
-                (threads == 128) ? record_sign<128>(cs, out, msgs) : record_sign<256>(cs, out, msgs);
+                (threads == 128) ? record_sign<128>(cs, out, msgs, sig) : record_sign<256>(cs, out, msgs, sig);
             else
                 (threads == 128) ? record_verify<128>(cs, reinterpret_cast<int *>(out), sig, msgs)
                                  : record_verify<256>(cs, reinterpret_cast<int *>(out), sig, msgs);
@@ -307,8 +307,9 @@ struct EngineImpl : EngineBase {
         return e == cudaSuccess ? CUDIL_OK : cudil_record_cuda_error(e, __FILE__, __LINE__);
     }
 
+    // d_rhop: randomized signing seeds, 64 bytes per item (dense, device); nullptr = deterministic
     int sign(uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes, const unsigned long long *off, const unsigned *mlen,
-             const unsigned *key, size_t n, cudaStream_t st) {
+             const unsigned *key, size_t n, cudaStream_t st, const uint8_t *d_rhop = nullptr) {
         if (n == 0) return CUDIL_OK;
         if (!d_sig || !off || !mlen || !key || n > max_items || n_sk == 0) return CUDIL_ERR_INVALID;
         if (!d_msgs) {
@@ -319,11 +320,13 @@ struct EngineImpl : EngineBase {
         if (((uintptr_t)d_msgs) & 7u) return CUDIL_ERR_INVALID;
         int rc = upload_meta(off, mlen, key, n, n_sk, msgs_bytes, true, st);
         if (rc) return rc;
-        if (!g_sign || g_sign_key[0] != d_sig || g_sign_key[1] != d_msgs) {
-            rc = capture(st, &g_sign, true, d_sig, nullptr, d_msgs);
+        if (!g_sign || g_sign_key[0] != d_sig || g_sign_key[1] != d_msgs || g_sign_key[2] != d_rhop) {
+            // for a signing graph the `sig` argument of capture carries the randomized-signing seeds
+            rc = capture(st, &g_sign, true, d_sig, d_rhop, d_msgs);
             if (rc) return rc;
             g_sign_key[0] = d_sig;
             g_sign_key[1] = d_msgs;
+            g_sign_key[2] = d_rhop;
         }
         CUDIL_LAUNCH(KID_FUSED_SIGN, st, cudaGraphLaunch(g_sign, st));
         CUDIL_CK_LAUNCH();

@@ -176,6 +176,7 @@ struct MsgRefs {
     const unsigned int *mlens;
     const unsigned int *key_idx;
     const unsigned int *order;
+    const uint8_t *rhoprime;  // randomized signing: 64 bytes per item (dense); nullptr = SHAKE256(K || mu)
 };
 
 template <int MODE>
@@ -196,6 +197,12 @@ __global__ void __launch_bounds__(kBlock) k_fused_prehash(const uint8_t *cache, 
         uint2 *out = reinterpret_cast<uint2 *>(items + (size_t)it * C::ITEM_BYTES);
 #pragma unroll
         for (int w = 0; w < 8; ++w) out[w] = mu[w];
+        if (mr.rhoprime) {
+            const uint8_t *rp = mr.rhoprime + (size_t)it * CRHBYTES;
+#pragma unroll 1
+            for (int b = 0; b < CRHBYTES; ++b) items[(size_t)it * C::ITEM_BYTES + 64 + b] = rp[b];
+            continue;
+        }
         uint2 key[4];
         ld_lanes(key, row + C::SK_KEY);
         keccak_zero(al, ah);

@@ -78,12 +78,16 @@ struct Impl {
     }
 
     // ---------------------------------------------------------------- sign
+    // rhop: optional caller-supplied rho' rows (64 bytes, rhop_pitch apart, memory kind in_kind) for
+    // randomized signing; nullptr = deterministic rho' = SHAKE256(K || mu).
     static int sign_setup(const uint8_t *m, size_t m_pitch, size_t mlen, const uint32_t *mlens, const uint8_t *sk,
-                          size_t sk_pitch, uint8_t *pool, size_t sp, size_t n, cudaStream_t st, cudaMemcpyKind in_kind) {
+                          size_t sk_pitch, uint8_t *pool, size_t sp, size_t n, cudaStream_t st, cudaMemcpyKind in_kind,
+                          const uint8_t *rhop = nullptr, size_t rhop_pitch = 0) {
         const int nn = (int)n;
         if (mlen) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::SG_MSG, sp, m, m_pitch, mlen, n, in_kind, st));
         CUDIL_CK(cudaMemcpy2DAsync(pool + LY::SG_SK, sp, sk, sk_pitch, PM::SK_BYTES, n, in_kind, st));
-        CUDIL_LAUNCH(KID_SIGN_PREHASH, st, k_sign_prehash<MODE><<<blocks_for(n, kItemBlock), kItemBlock, 0, st>>>(pool, sp, mlen, mlens, nn));
+        if (rhop) CUDIL_CK(cudaMemcpy2DAsync(pool + LY::SG_RHOP, sp, rhop, rhop_pitch, CRHBYTES, n, in_kind, st));
+        CUDIL_LAUNCH(KID_SIGN_PREHASH, st, k_sign_prehash<MODE><<<blocks_for(n, kItemBlock), kItemBlock, 0, st>>>(pool, sp, mlen, mlens, nn, rhop ? 1 : 0));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_EXPAND_A, st, k_expand_a<MODE><<<blocks_for(n * K * L), kBlock, 0, st>>>(pool, sp, LY::SG_SK + PM::SK_RHO, LY::sg_mat(mlen), nn));
         CUDIL_CK_LAUNCH();
@@ -111,7 +115,8 @@ struct Impl {
     static int sign(uint8_t *sig, size_t sig_pitch, size_t *siglen, const uint8_t *m, size_t m_pitch, size_t mlen,
                     const uint8_t *sk, size_t sk_pitch, uint8_t *pool, size_t sp, uint8_t *tpool, size_t tp,
                     cudil_task_lut *lut, size_t T, size_t n, cudaStream_t st, cudaMemcpyKind in_kind,
-                    cudaMemcpyKind out_kind, const uint32_t *mlens = nullptr) {
+                    cudaMemcpyKind out_kind, const uint32_t *mlens = nullptr, const uint8_t *rhop = nullptr,
+                    size_t rhop_pitch = 0) {
         if (siglen) *siglen = PM::SIG_BYTES;
         if (n == 0) return CUDIL_OK;
         if (!sig || !sk || (!m && mlen) || !pool || !tpool || !lut || T == 0 || n > 65536) return CUDIL_ERR_INVALID;
@@ -121,7 +126,8 @@ struct Impl {
         if (!lut->sign_lut || lut->sign_lut_len != n || !lut->h_exec_lut || !lut->h_done_lut || !lut->h_copy_lut ||
             !lut->d_exec_lut || !lut->d_done_lut || !lut->d_copy_lut)
             return CUDIL_ERR_INVALID;
-        int rc = sign_setup(m, m_pitch, mlen, mlens, sk, sk_pitch, pool, sp, n, st, in_kind);
+        if (rhop && rhop_pitch < (size_t)CRHBYTES) return CUDIL_ERR_INVALID;
+        int rc = sign_setup(m, m_pitch, mlen, mlens, sk, sk_pitch, pool, sp, n, st, in_kind, rhop, rhop_pitch);
         if (rc) return rc;
 
         cudil_sign_lut_element *sl = lut->sign_lut;

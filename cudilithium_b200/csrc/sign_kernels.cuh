@@ -23,9 +23,10 @@ constexpr int kItemBlock = 32;          // threads per block for thread-per-item
 
 // ------------------------------------------------------------------ per-item setup
 
+// rhop_given: rho' was placed in the row by the caller (randomized signing), only mu is computed.
 template <int MODE>
 __global__ void __launch_bounds__(kBlock) k_sign_prehash(uint8_t *pool, size_t pitch, size_t mlen, const uint32_t *mlens,
-                                                         int n) {
+                                                         int n, int rhop_given) {
     using LY = Layout<MODE>;
     const int it = blockIdx.x * blockDim.x + threadIdx.x;
     if (it >= n) return;
@@ -41,6 +42,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_prehash(uint8_t *pool, size_t p
     uint2 *mu_out = reinterpret_cast<uint2 *>(row + LY::SG_MU);
 #pragma unroll
     for (int w = 0; w < 8; ++w) mu_out[w] = mu[w];
+    if (rhop_given) return;
     // rho' = SHAKE256(K || mu, 64): 96 bytes, one block
     uint2 key[4];
     ld_lanes(key, row + LY::SG_SK + P<MODE>::SK_KEY);

@@ -100,11 +100,18 @@ class Engine:
         n = d_pk.numel() // self.params.pk_bytes
         check(lib.cudil_engine_set_public_keys(self.h, d_pk.data_ptr(), n, _sp(stream)), "set_public_keys")
 
-    def sign(self, d_sig: torch.Tensor, d_msgs: torch.Tensor, offsets, mlens, key_idx, stream=None):
+    def sign(self, d_sig: torch.Tensor, d_msgs: torch.Tensor, offsets, mlens, key_idx, stream=None,
+             d_rhoprime: torch.Tensor | None = None):
+        """d_rhoprime: optional device tensor of 64 random bytes per item (randomized signing)."""
         offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
         mlens = np.ascontiguousarray(mlens, dtype=np.uint32)
         key_idx = np.ascontiguousarray(key_idx, dtype=np.uint32)
         n = len(mlens)
+        if d_rhoprime is not None:
+            check(lib.cudil_engine_sign_randomized(self.h, d_sig.data_ptr(), d_msgs.data_ptr(), d_msgs.numel(),
+                                                   offsets.ctypes.data, mlens.ctypes.data, key_idx.ctypes.data,
+                                                   d_rhoprime.data_ptr(), n, _sp(stream)), "cudil_engine_sign_randomized")
+            return
         check(lib.cudil_engine_sign(self.h, d_sig.data_ptr(), d_msgs.data_ptr(), d_msgs.numel(), offsets.ctypes.data,
                                     mlens.ctypes.data, key_idx.ctypes.data, n, _sp(stream)), "cudil_engine_sign")
 
@@ -138,11 +145,14 @@ class Engine:
         return {"claim": cyc[0], "keccak": cyc[1], "ntt": cyc[2], "total": cyc[3], "iterations": it.value}
 
     # ---- numpy conveniences (synchronous)
-    def sign_np(self, msgs, key_idx) -> np.ndarray:
+    def sign_np(self, msgs, key_idx, rhoprime: np.ndarray | None = None) -> np.ndarray:
         d_msgs, offs, lens = pack_messages(msgs)
         n = len(lens)
         d_sig = torch.empty(max(n, 1) * self.params.sig_bytes, dtype=torch.uint8, device="cuda")
-        self.sign(d_sig, d_msgs, offs, lens, key_idx)
+        d_rp = None
+        if rhoprime is not None:
+            d_rp = torch.from_numpy(np.ascontiguousarray(rhoprime, dtype=np.uint8).reshape(-1)).cuda()
+        self.sign(d_sig, d_msgs, offs, lens, key_idx, d_rhoprime=d_rp)
         torch.cuda.synchronize()
         self.last_status()
         return d_sig.cpu().numpy()[: n * self.params.sig_bytes].reshape(n, self.params.sig_bytes)

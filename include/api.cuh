@@ -19,6 +19,11 @@
  * missing buffer) or a CUDA failure is reported: crypto_sign_keypair / crypto_sign_signature
  * return the negative cudilithium status, crypto_sign_verify sets every ret[i] = -1.
  *
+ * Defining DILITHIUM_RANDOMIZED_SIGNING (as for the reference) makes crypto_sign_signature draw the
+ * 64-byte rho' of every message from /dev/urandom and sign with cudil_sign_randomized.  The
+ * rho' buffer is pageable host memory, so the reference's asynchronous upload of it becomes a
+ * synchronous copy; every other step is unchanged.
+ *
  * The parameter macros keep the names of the Dilithium specification's reference code, which the
  * reference's params.h uses, so pool sizes computed from them are the reference's.
  */
@@ -28,6 +33,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cstdio>
 #include <vector>
 
 #include "cudilithium.h"
@@ -129,6 +135,17 @@ inline int crypto_sign_keypair(uint8_t *pk, uint8_t *sk, uint8_t *d_keypair_mem_
                          (void *)stream, rand_index);
 }
 
+#ifdef DILITHIUM_RANDOMIZED_SIGNING
+// rho' from the operating system's random source, as the reference's randombytes (src/api.cu:143-148)
+inline bool cudil_os_random(uint8_t *out, size_t n) {
+    FILE *f = std::fopen("/dev/urandom", "rb");
+    if (!f) return false;
+    const bool ok = std::fread(out, 1, n, f) == n;
+    std::fclose(f);
+    return ok;
+}
+#endif
+
 inline int crypto_sign_signature(uint8_t *sig, size_t sig_pitch, size_t *siglen, const uint8_t *m, size_t m_pitch,
                                  size_t mlen, const uint8_t *sk, uint8_t *d_sign_mem_pool,
                                  size_t d_sign_mem_pool_pitch, uint8_t *d_temp_mem_pool,
@@ -143,9 +160,17 @@ inline int crypto_sign_signature(uint8_t *sig, size_t sig_pitch, size_t *siglen,
     c.d_exec_lut = lut.d_exec_lut;
     c.d_done_lut = lut.d_done_lut;
     c.d_copy_lut = reinterpret_cast<cudil_copy_lut_element *>(lut.d_copy_lut);
+#ifdef DILITHIUM_RANDOMIZED_SIGNING
+    std::vector<uint8_t> rhoprime(batch_size * CRHBYTES);
+    if (batch_size && !cudil_os_random(rhoprime.data(), rhoprime.size())) return CUDIL_ERR_INVALID;
+    return cudil_sign_randomized(DILITHIUM_MODE, sig, sig_pitch, siglen, m, m_pitch, mlen, sk, rhoprime.data(), CRHBYTES,
+                                 d_sign_mem_pool, d_sign_mem_pool_pitch, d_temp_mem_pool, d_temp_mem_pool_pitch, &c,
+                                 exec_threshold, batch_size, (void *)stream);
+#else
     return cudil_sign(DILITHIUM_MODE, sig, sig_pitch, siglen, m, m_pitch, mlen, sk, d_sign_mem_pool,
                       d_sign_mem_pool_pitch, d_temp_mem_pool, d_temp_mem_pool_pitch, &c, exec_threshold, batch_size,
                       (void *)stream);
+#endif
 }
 
 inline void crypto_sign_verify(int *ret, const uint8_t *sig, size_t sig_pitch, size_t siglen, const uint8_t *m,

@@ -100,6 +100,21 @@ int cudil_verify(int mode, int *ret, const uint8_t *sig, size_t sig_pitch, size_
                  size_t m_pitch, size_t mlen, const uint8_t *pk, uint8_t *d_verify_pool, size_t verify_pool_pitch,
                  size_t batch_size, void *stream);
 
+/* Randomized signing (the reference's DILITHIUM_RANDOMIZED_SIGNING, src/api.cu:143-148): the
+ * per-message seed rho' is 64 caller-supplied random bytes (row i at rhoprime + i * rhoprime_pitch)
+ * instead of SHAKE256(K || mu).  The caller draws them from its random source (the api.cuh shim
+ * uses the operating system's); everything else is cudil_sign / cudil_sign_dev.  Given rho', the
+ * signature is deterministic (the smallest accepted nonce), so it can be checked bit for bit. */
+int cudil_sign_randomized(int mode, uint8_t *sig, size_t sig_pitch, size_t *siglen, const uint8_t *m, size_t m_pitch,
+                          size_t mlen, const uint8_t *sk, const uint8_t *rhoprime, size_t rhoprime_pitch,
+                          uint8_t *d_sign_pool, size_t sign_pool_pitch, uint8_t *d_temp_pool, size_t temp_pool_pitch,
+                          cudil_task_lut *lut, size_t exec_threshold, size_t batch_size, void *stream);
+int cudil_sign_dev_randomized(int mode, uint8_t *d_sig, size_t sig_pitch, const uint8_t *d_m, size_t m_pitch,
+                              size_t mlen, const uint8_t *d_sk, const uint8_t *d_rhoprime, size_t rhoprime_pitch,
+                              uint8_t *d_sign_pool, size_t sign_pool_pitch, uint8_t *d_temp_pool,
+                              size_t temp_pool_pitch, cudil_task_lut *lut, size_t exec_threshold, size_t batch_size,
+                              void *stream);
+
 /* Device-resident variants: every data pointer is device memory (m, sk, pk, sig, seeds, ret),
  * nothing crosses PCIe except the sign scheduler's per-round flags. */
 int cudil_keypair_dev(int mode, uint8_t *d_pk, uint8_t *d_sk, const uint8_t *d_seeds, uint8_t *d_keypair_pool,
@@ -178,6 +193,11 @@ int cudil_engine_set_public_keys(cudil_engine *e, const uint8_t *d_pk, size_t nk
 int cudil_engine_sign(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
                       const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
                       void *stream);
+/* Randomized signing through the engine: d_rhoprime holds 64 random bytes per item (dense, device
+ * memory), used as rho' instead of SHAKE256(K || mu). */
+int cudil_engine_sign_randomized(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
+                                 const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx,
+                                 const uint8_t *d_rhoprime, size_t n, void *stream);
 int cudil_engine_verify(cudil_engine *e, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
                         const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
                         void *stream);

@@ -44,6 +44,7 @@ def _load():
         "ora_shake256": (None, [P8, c_size_t, P8, c_size_t]),
         "ora_keypair_from_seed": (c_int, [c_int, P8, P8, P8]),
         "ora_sign": (c_int, [c_int, P8, P8, c_size_t, P8, POINTER(c_int)]),
+        "ora_sign_rhoprime": (c_int, [c_int, P8, P8, c_size_t, P8, P8, POINTER(c_int)]),
         "ora_verify": (c_int, [c_int, P8, c_size_t, P8, c_size_t, P8]),
         "ora_seed_from_ctr": (None, [P8, c_uint64]),
         "ora_keypair_batch": (c_int, [c_int, P8, P8, c_size_t, c_uint64, c_int]),
@@ -135,6 +136,20 @@ def sign_batch(mode: int, m: np.ndarray, sk: np.ndarray, mlens=None, nthreads: i
     assert lib.ora_sign_batch(mode, _p(sig), p.sig_bytes, _p(m), stride, _p(ml), _p(sk), p.sk_bytes, n, nthreads,
                               _p(att)) == 0
     return (sig, att) if return_attempts else sig
+
+
+def sign_rhoprime(mode: int, m: bytes, sk: np.ndarray, rhoprime: bytes) -> np.ndarray:
+    """Randomized signing with a given rho' (64 bytes) instead of SHAKE256(K || mu)
+    (reference src/api.cu:143-148)."""
+    p = params(mode)
+    sig = np.zeros(p.sig_bytes, np.uint8)
+    mb = np.frombuffer(bytes(m) + b"\0", np.uint8)
+    skb = np.ascontiguousarray(sk, dtype=np.uint8).reshape(-1)
+    rp = np.frombuffer(bytes(rhoprime), np.uint8)
+    assert rp.size == 64
+    att = ctypes.c_int(0)
+    assert lib.ora_sign_rhoprime(mode, _p(sig), _p(mb), len(m), _p(skb), _p(rp), ctypes.byref(att)) == 0
+    return sig
 
 
 def verify_batch(mode: int, sig: np.ndarray, m: np.ndarray, pk: np.ndarray, mlens=None, siglen=None,

@@ -15,9 +15,9 @@ LIBDIR = ROOT / "cudilithium_b200"
 CUDA = Path("/usr/local/cuda")
 
 
-def build_shim(mode: int, out: Path) -> Path:
+def build_shim(mode: int, out: Path, extra=()) -> Path:
     exe = out / f"kat_shim{mode}"
-    cmd = ["g++", "-O1", "-std=c++17", f"-DDILITHIUM_MODE={mode}", f"-I{ROOT / 'include'}",
+    cmd = ["g++", "-O1", "-std=c++17", f"-DDILITHIUM_MODE={mode}", *extra, f"-I{ROOT / 'include'}",
            f"-I{CUDA / 'include'}", str(SRC), "-o", str(exe), f"-L{LIBDIR}", "-lcudilithium_b200",
            f"-Wl,-rpath,{LIBDIR}", f"-L{CUDA / 'lib64'}", "-lcudart", f"-Wl,-rpath,{CUDA / 'lib64'}"]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
@@ -31,6 +31,13 @@ def test_api_shim_compiles_and_links(tmp_path, mode):
         pytest.skip("library not built")
     exe = build_shim(mode, tmp_path)
     assert exe.exists()
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_api_shim_randomized_compiles_and_links(tmp_path):
+    if not (LIBDIR / "libcudilithium_b200.so").exists():
+        pytest.skip("library not built")
+    assert build_shim(5, tmp_path, extra=["-DDILITHIUM_RANDOMIZED_SIGNING"]).exists()
 
 
 @pytest.mark.gpu
