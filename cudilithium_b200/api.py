@@ -183,6 +183,28 @@ class Dilithium:
         sig = hsig.numpy()[: n * self.CRYPTO_BYTES].reshape(n, self.CRYPTO_BYTES).copy()
         return (sig, lut) if return_lut else sig
 
+    def sig_check(self, sig: np.ndarray, sig_pitch: int | None = None) -> np.ndarray:
+        """Parse step on the GPU (cudil_sig_check): per signature, bit 0 = bad hint encoding,
+        bit 1 = a z coefficient out of range."""
+        sig = np.ascontiguousarray(sig, dtype=np.uint8)
+        n = sig.shape[0]
+        pitch = sig_pitch or sig.shape[1]
+        d_sig = torch.from_numpy(sig.reshape(-1)).cuda()
+        d_st = torch.full((max(n, 1),), -7, dtype=torch.int32, device="cuda")
+        check(lib.cudil_sig_check(self.mode, _ptr(d_st), _ptr(d_sig), pitch, n, None), "cudil_sig_check")
+        torch.cuda.synchronize()
+        return d_st.cpu().numpy()[:n]
+
+    def sk_check(self, sk: np.ndarray) -> np.ndarray:
+        """Parse step on the GPU (cudil_sk_check): 1 where an s1/s2 eta field is out of range."""
+        sk = np.ascontiguousarray(sk, dtype=np.uint8)
+        n = sk.shape[0]
+        d_sk = torch.from_numpy(sk.reshape(-1)).cuda()
+        d_st = torch.full((max(n, 1),), -7, dtype=torch.int32, device="cuda")
+        check(lib.cudil_sk_check(self.mode, _ptr(d_st), _ptr(d_sk), n, None), "cudil_sk_check")
+        torch.cuda.synchronize()
+        return d_st.cpu().numpy()[:n]
+
     def verify(self, sig: np.ndarray, m: np.ndarray, pk: np.ndarray, siglen: int | None = None) -> np.ndarray:
         m = np.ascontiguousarray(m, dtype=np.uint8)
         n, mlen = m.shape

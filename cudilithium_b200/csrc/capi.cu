@@ -1,10 +1,12 @@
 // extern "C" boundary: run-time parameter-set dispatch onto the per-mode instantiations, pool row
 // size queries, and the NTT microbenchmark kernel.
+#include <climits>
 #include <cstdio>
 #include <cuda_runtime.h>
 
 #include "../../include/cudilithium.h"
 #include "host_impl.cuh"
+#include "parse_kernels.cuh"
 #include "profiling.cuh"
 
 namespace cudil {
@@ -231,6 +233,51 @@ int cudil_verify_dev_varlen(int mode, int *d_ret, const uint8_t *d_sig, size_t s
     CUDIL_DISPATCH(mode, I::verify(d_ret, d_sig, sig_pitch, siglen, d_m, m_pitch, max_mlen, d_pk, I::PM::PK_BYTES, d_pool,
                                    pitch, batch, (cudaStream_t)stream, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice,
                                    d_mlens))
+}
+
+}  // extern "C"
+
+namespace {
+template <int MODE>
+int sig_check_impl(int *d_status, const uint8_t *d_sig, size_t sig_pitch, size_t n, cudaStream_t st) {
+    using namespace cudil;
+    if (n == 0) return CUDIL_OK;
+    if (!d_status || !d_sig || sig_pitch < (size_t)P<MODE>::SIG_BYTES || n > (size_t)INT_MAX / 32) return CUDIL_ERR_INVALID;
+    CUDIL_LAUNCH(KID_SIG_CHECK, st, k_sig_check<MODE><<<blocks_for(n * 32), kBlock, 0, st>>>(d_status, d_sig, sig_pitch, (int)n));
+    CUDIL_CK_LAUNCH();
+    return CUDIL_OK;
+}
+template <int MODE>
+int sk_check_impl(int *d_status, const uint8_t *d_sk, size_t n, cudaStream_t st) {
+    using namespace cudil;
+    if (n == 0) return CUDIL_OK;
+    if (!d_status || !d_sk || n > (size_t)INT_MAX / 32) return CUDIL_ERR_INVALID;
+    CUDIL_LAUNCH(KID_SK_CHECK, st, k_sk_check<MODE><<<blocks_for(n * 32), kBlock, 0, st>>>(d_status, d_sk, (int)n));
+    CUDIL_CK_LAUNCH();
+    return CUDIL_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int cudil_sig_check(int mode, int *d_status, const uint8_t *d_sig, size_t sig_pitch, size_t batch, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (mode) {
+        case 2: return sig_check_impl<2>(d_status, d_sig, sig_pitch, batch, st);
+        case 3: return sig_check_impl<3>(d_status, d_sig, sig_pitch, batch, st);
+        case 5: return sig_check_impl<5>(d_status, d_sig, sig_pitch, batch, st);
+        default: return CUDIL_ERR_INVALID;
+    }
+}
+
+int cudil_sk_check(int mode, int *d_status, const uint8_t *d_sk, size_t batch, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (mode) {
+        case 2: return sk_check_impl<2>(d_status, d_sk, batch, st);
+        case 3: return sk_check_impl<3>(d_status, d_sk, batch, st);
+        case 5: return sk_check_impl<5>(d_status, d_sk, batch, st);
+        default: return CUDIL_ERR_INVALID;
+    }
 }
 
 int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t npolys, void *stream) {

@@ -34,6 +34,8 @@ enum KernelId : int {
     KID_FUSED_SCHED,
     KID_CACHE_SK,
     KID_CACHE_PK,
+    KID_SIG_CHECK,
+    KID_SK_CHECK,
     KID_COUNT
 };
 
@@ -42,7 +44,8 @@ inline const char *kernel_name(int id) {
         "k_kp_seed", "k_kp_main", "k_kp_tr", "k_sign_prehash", "k_expand_a", "k_sign_unpack_ntt",
         "k_sign_expand_mask", "k_sign_compute_w", "k_sign_challenge", "k_sign_reject", "k_sig_copy",
         "k_verify_prepare", "k_verify_w", "k_verify_final", "k_ntt_mul", "k_alu_peak",
-        "k_fused_sign (graph)", "k_fused_verify (graph)", "k_fused_sched", "k_cache_sk", "k_cache_pk"};
+        "k_fused_sign (graph)", "k_fused_verify (graph)", "k_fused_sched", "k_cache_sk", "k_cache_pk",
+        "k_sig_check", "k_sk_check"};
     return (id >= 0 && id < KID_COUNT) ? names[id] : "?";
 }
 

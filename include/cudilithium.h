@@ -115,6 +115,16 @@ int cudil_sign_dev_randomized(int mode, uint8_t *d_sig, size_t sig_pitch, const 
                               size_t temp_pool_pitch, cudil_task_lut *lut, size_t exec_threshold, size_t batch_size,
                               void *stream);
 
+/* Batched well-formedness checks, a parse step of their own (extends the reference, whose hint
+ * checks run inside verification, src/verify.cu:51-93).  All pointers are device memory; results
+ * are asynchronous on `stream`.
+ * cudil_sig_check: d_status[i] bit 0 = hint encoding invalid, bit 1 = a z coefficient with
+ *   |z| >= gamma1 - beta; 0 = well formed (verification still decides validity).
+ * cudil_sk_check: d_status[i] = 1 if an s1 / s2 coefficient field lies outside [0, 2 eta] (dense
+ *   rows of sk_bytes).  Public keys need no check: every pk_bytes string is a valid encoding. */
+int cudil_sig_check(int mode, int *d_status, const uint8_t *d_sig, size_t sig_pitch, size_t batch_size, void *stream);
+int cudil_sk_check(int mode, int *d_status, const uint8_t *d_sk, size_t batch_size, void *stream);
+
 /* Device-resident variants: every data pointer is device memory (m, sk, pk, sig, seeds, ret),
  * nothing crosses PCIe except the sign scheduler's per-round flags. */
 int cudil_keypair_dev(int mode, uint8_t *d_pk, uint8_t *d_sk, const uint8_t *d_seeds, uint8_t *d_keypair_pool,

@@ -561,6 +561,57 @@ int ora_sign(int mode, uint8_t *sig, const uint8_t *m, size_t mlen, const uint8_
     return ora_sign_rhoprime(mode, sig, m, mlen, sk, NULL, attempts);
 }
 
+/* ---------------------------------------------------------------- well-formedness checks */
+
+/* Signature parse step: bit 0 = hint encoding invalid (per-poly end counts non-decreasing and at
+ * most omega, positions strictly increasing inside a poly, unused slots zero: src/verify.cu:51-93),
+ * bit 1 = a z coefficient with |z| >= gamma1 - beta (the z check of src/verify.cu:98-121). */
+int ora_sig_check(int mode, const uint8_t *sig) {
+    ora_params p;
+    int32_t z[N];
+    const uint8_t *hs;
+    int i, j, kk, st = 0;
+    if (ora_params_get(mode, &p)) return -1;
+    hs = sig + 32 + p.l * p.polyz_packed;
+    kk = 0;
+    for (i = 0; i < p.k && !(st & 1); i++) {
+        if (hs[p.omega + i] < kk || hs[p.omega + i] > p.omega) {
+            st |= 1;
+            break;
+        }
+        for (j = kk; j < hs[p.omega + i]; j++)
+            if (j > kk && hs[j] <= hs[j - 1]) st |= 1;
+        kk = hs[p.omega + i];
+    }
+    if (!(st & 1))
+        for (j = kk; j < p.omega; j++)
+            if (hs[j]) st |= 1;
+    for (j = 0; j < p.l; j++) {
+        unpack_offset(z, sig + 32 + j * p.polyz_packed, p.gamma1, z_bits(&p));
+        if (chknorm(z, p.gamma1 - p.beta)) st |= 2;
+    }
+    return st;
+}
+
+/* Secret-key parse step: bit 0 = an s1 / s2 coefficient field outside [0, 2 eta] (the eta
+ * encoding of src/keypair.cu:116-130 stores eta - s). */
+int ora_sk_check(int mode, const uint8_t *sk) {
+    ora_params p;
+    const uint8_t *o;
+    int j, c, eb, st = 0;
+    if (ora_params_get(mode, &p)) return -1;
+    eb = eta_bits(&p);
+    o = sk + 96;
+    for (j = 0; j < p.l + p.k; j++, o += p.polyeta_packed)
+        for (c = 0; c < N; c++) {
+            const int bit = c * eb;
+            uint32_t v = (uint32_t)o[bit >> 3] >> (bit & 7);
+            if ((bit & 7) + eb > 8) v |= (uint32_t)o[(bit >> 3) + 1] << (8 - (bit & 7));
+            if ((int)(v & ((1u << eb) - 1u)) > 2 * p.eta) st |= 1;
+        }
+    return st;
+}
+
 /* ---------------------------------------------------------------- verify */
 
 int ora_verify(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen, const uint8_t *pk) {

@@ -57,6 +57,8 @@ int ora_sign(int mode, uint8_t *sig, const uint8_t *m, size_t mlen, const uint8_
 int ora_sign_rhoprime(int mode, uint8_t *sig, const uint8_t *m, size_t mlen, const uint8_t *sk,
                       const uint8_t *rhoprime, int *attempts);
 int ora_verify(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen, const uint8_t *pk);
+int ora_sig_check(int mode, const uint8_t *sig);
+int ora_sk_check(int mode, const uint8_t *sk);
 
 /* Batched forms (OpenMP over items; nthreads <= 0 means all available). */
 void ora_seed_from_ctr(uint8_t seed[32], uint64_t ctr);

@@ -45,6 +45,8 @@ def _load():
         "ora_keypair_from_seed": (c_int, [c_int, P8, P8, P8]),
         "ora_sign": (c_int, [c_int, P8, P8, c_size_t, P8, POINTER(c_int)]),
         "ora_sign_rhoprime": (c_int, [c_int, P8, P8, c_size_t, P8, P8, POINTER(c_int)]),
+        "ora_sig_check": (c_int, [c_int, P8]),
+        "ora_sk_check": (c_int, [c_int, P8]),
         "ora_verify": (c_int, [c_int, P8, c_size_t, P8, c_size_t, P8]),
         "ora_seed_from_ctr": (None, [P8, c_uint64]),
         "ora_keypair_batch": (c_int, [c_int, P8, P8, c_size_t, c_uint64, c_int]),
@@ -150,6 +152,18 @@ def sign_rhoprime(mode: int, m: bytes, sk: np.ndarray, rhoprime: bytes) -> np.nd
     att = ctypes.c_int(0)
     assert lib.ora_sign_rhoprime(mode, _p(sig), _p(mb), len(m), _p(skb), _p(rp), ctypes.byref(att)) == 0
     return sig
+
+
+def sig_check(mode: int, sig: np.ndarray) -> np.ndarray:
+    """Per-signature parse status: bit 0 bad hint encoding, bit 1 z out of range."""
+    sig = np.ascontiguousarray(sig, dtype=np.uint8).reshape(-1, params(mode).sig_bytes)
+    return np.array([lib.ora_sig_check(mode, _p(np.ascontiguousarray(r))) for r in sig], dtype=np.int32)
+
+
+def sk_check(mode: int, sk: np.ndarray) -> np.ndarray:
+    """Per-key parse status: bit 0 an s1/s2 eta field out of range."""
+    sk = np.ascontiguousarray(sk, dtype=np.uint8).reshape(-1, params(mode).sk_bytes)
+    return np.array([lib.ora_sk_check(mode, _p(np.ascontiguousarray(r))) for r in sk], dtype=np.int32)
 
 
 def verify_batch(mode: int, sig: np.ndarray, m: np.ndarray, pk: np.ndarray, mlens=None, siglen=None,

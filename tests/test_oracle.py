@@ -86,3 +86,24 @@ def test_oracle_negative_cases(oracle, mode):
     ret = oracle.verify_batch(mode, bad, m2, pk)
     assert list(ret[:4]) == [-1, -1, -1, -1]
     assert np.all(oracle.verify_batch(mode, sig, m, pk, siglen=p.sig_bytes - 1) == -1)
+
+
+@pytest.mark.parametrize("mode", [2, 3, 5])
+def test_oracle_parse_checks(oracle, mode):
+    """The parse checks accept genuine encodings and flag malformed hints / z / eta fields; a
+    flagged signature never verifies."""
+    p = oracle.params(mode)
+    pk, sk = oracle.keypair_batch(mode, 6, rand_index=77 + mode)
+    m = oracle.messages_from_ctr(6, 32)
+    sig = oracle.sign_batch(mode, m, sk)
+    assert np.all(oracle.sig_check(mode, sig) == 0) and np.all(oracle.sk_check(mode, sk) == 0)
+    h0 = 32 + p.l * p.polyz_packed
+    bad = sig.copy()
+    bad[0, h0 + p.omega + p.k - 1] = p.omega + 1
+    bad[1, 32:35] = 0
+    st = oracle.sig_check(mode, bad)
+    assert st[0] & 1 and st[1] & 2
+    assert np.all(oracle.verify_batch(mode, bad[:2], m[:2], pk[:2]) == -1)
+    bsk = sk.copy()
+    bsk[3, 96] = 0xFF
+    assert oracle.sk_check(mode, bsk)[3] == 1
