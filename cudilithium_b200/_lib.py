@@ -97,6 +97,11 @@ SIGNATURES = {
                              c_void_p, c_size_t, c_size_t, c_void_p]),
     "cudil_verify_dev": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
                                  c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
+    "cudil_crypto_sign": (c_int, [c_int, c_void_p, c_size_t, POINTER(c_size_t), c_void_p, c_size_t, c_size_t, c_void_p,
+                                  c_void_p, c_size_t, c_void_p, c_size_t, POINTER(cudil_task_lut), c_size_t, c_size_t,
+                                  c_void_p]),
+    "cudil_crypto_sign_open": (c_int, [c_int, c_void_p, c_size_t, POINTER(c_size_t), c_void_p, c_void_p, c_size_t,
+                                       c_size_t, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
     "cudil_sig_check": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
     "cudil_sk_check": (c_int, [c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
     "cudil_ntt_mul": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),

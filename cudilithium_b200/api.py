@@ -183,6 +183,46 @@ class Dilithium:
         sig = hsig.numpy()[: n * self.CRYPTO_BYTES].reshape(n, self.CRYPTO_BYTES).copy()
         return (sig, lut) if return_lut else sig
 
+    def crypto_sign(self, m: np.ndarray, sk: np.ndarray, exec_threshold: int = 2048) -> np.ndarray:
+        """Signed messages sm = sig || m for every row of m (cudil_crypto_sign)."""
+        m = np.ascontiguousarray(m, dtype=np.uint8)
+        n, mlen = m.shape
+        smb = self.CRYPTO_BYTES + mlen
+        pool, sp = alloc_pool(self.sign_row_bytes(mlen), n)
+        tpool, tp = alloc_pool(self.sign_temp_row_bytes(), exec_threshold)
+        lut = TaskLut(n, exec_threshold)
+        hm = pinned(max(m.size, 1))
+        hm.numpy()[: m.size] = m.reshape(-1)
+        hsk = pinned(n * self.CRYPTO_SECRETKEYBYTES)
+        hsk.numpy()[: n * self.CRYPTO_SECRETKEYBYTES] = np.ascontiguousarray(sk, dtype=np.uint8).reshape(-1)
+        hsm = pinned(n * smb)
+        smlen = ctypes.c_size_t(0)
+        check(lib.cudil_crypto_sign(self.mode, _ptr(hsm), smb, ctypes.byref(smlen), _ptr(hm), mlen, mlen, _ptr(hsk),
+                                    _ptr(pool), sp, _ptr(tpool), tp, ctypes.byref(lut.c), exec_threshold, n, None),
+              "cudil_crypto_sign")
+        torch.cuda.synchronize()
+        assert smlen.value == smb
+        return hsm.numpy()[: n * smb].reshape(n, smb).copy()
+
+    def crypto_sign_open(self, sm: np.ndarray, pk: np.ndarray):
+        """(messages, ret) for every row of sm (cudil_crypto_sign_open); invalid rows give ret -1
+        and a zeroed message."""
+        sm = np.ascontiguousarray(sm, dtype=np.uint8)
+        n, smlen = sm.shape
+        mlen = max(smlen - self.CRYPTO_BYTES, 0)
+        pool, pitch = alloc_pool(self.verify_row_bytes(mlen), n)
+        hsm = pinned(max(sm.size, 1))
+        hsm.numpy()[: sm.size] = sm.reshape(-1)
+        hpk = pinned(n * self.CRYPTO_PUBLICKEYBYTES)
+        hpk.numpy()[: n * self.CRYPTO_PUBLICKEYBYTES] = np.ascontiguousarray(pk, dtype=np.uint8).reshape(-1)
+        hm = pinned(max(n * mlen, 1))
+        hret = pinned(n * 4)
+        ml = ctypes.c_size_t(12345)
+        check(lib.cudil_crypto_sign_open(self.mode, _ptr(hm), max(mlen, 1), ctypes.byref(ml), _ptr(hret), _ptr(hsm),
+                                         smlen, smlen, _ptr(hpk), _ptr(pool), pitch, n, None), "cudil_crypto_sign_open")
+        ret = hret.numpy()[: n * 4].view(np.int32).copy()
+        return hm.numpy()[: n * mlen].reshape(n, mlen).copy(), ret, ml.value
+
     def sig_check(self, sig: np.ndarray, sig_pitch: int | None = None) -> np.ndarray:
         """Parse step on the GPU (cudil_sig_check): per signature, bit 0 = bad hint encoding,
         bit 1 = a z coefficient out of range."""

@@ -2,6 +2,7 @@
 // size queries, and the NTT microbenchmark kernel.
 #include <climits>
 #include <cstdio>
+#include <cstring>
 #include <cuda_runtime.h>
 
 #include "../../include/cudilithium.h"
@@ -207,6 +208,53 @@ int cudil_verify(int mode, int *ret, const uint8_t *sig, size_t sig_pitch, size_
                  void *stream) {
     CUDIL_DISPATCH(mode, I::verify(ret, sig, sig_pitch, siglen, m, m_pitch, mlen, pk, I::PM::PK_BYTES, d_pool, pitch,
                                    batch, (cudaStream_t)stream, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost))
+}
+
+int cudil_crypto_sign(int mode, uint8_t *sm, size_t sm_pitch, size_t *smlen, const uint8_t *m, size_t m_pitch,
+                      size_t mlen, const uint8_t *sk, uint8_t *d_sign_pool, size_t sign_pitch, uint8_t *d_temp_pool,
+                      size_t temp_pitch, cudil_task_lut *lut, size_t exec_threshold, size_t batch, void *stream) {
+    cudil_params p;
+    if (cudil_get_params(mode, &p) != CUDIL_OK) return CUDIL_ERR_INVALID;
+    const size_t sb = (size_t)p.sig_bytes;
+    if (smlen) *smlen = sb + mlen;
+    if (batch == 0) return CUDIL_OK;
+    if (!sm || (mlen && !m) || sm_pitch < sb + mlen) return CUDIL_ERR_INVALID;
+    // message behind the signature slot first (memmove: m may already sit inside sm), then sign
+    // with the message read from its place in sm and the signature written in front of it
+    for (size_t i = 0; i < batch && mlen; ++i) std::memmove(sm + i * sm_pitch + sb, m + i * m_pitch, mlen);
+    return cudil_sign(mode, sm, sm_pitch, nullptr, sm + sb, sm_pitch, mlen, sk, d_sign_pool, sign_pitch, d_temp_pool,
+                      temp_pitch, lut, exec_threshold, batch, stream);
+}
+
+int cudil_crypto_sign_open(int mode, uint8_t *m, size_t m_pitch, size_t *mlen, int *ret, const uint8_t *sm,
+                           size_t sm_pitch, size_t smlen, const uint8_t *pk, uint8_t *d_verify_pool, size_t verify_pitch,
+                           size_t batch, void *stream) {
+    cudil_params p;
+    if (cudil_get_params(mode, &p) != CUDIL_OK) return CUDIL_ERR_INVALID;
+    const size_t sb = (size_t)p.sig_bytes;
+    if (batch == 0) return CUDIL_OK;
+    if (!ret || !m || !sm || !mlen) return CUDIL_ERR_INVALID;
+    if (smlen < sb) {
+        *mlen = 0;
+        for (size_t i = 0; i < batch; ++i) ret[i] = -1;
+        return CUDIL_OK;
+    }
+    const size_t ml = smlen - sb;
+    if (sm_pitch < smlen || (ml && m_pitch < ml)) return CUDIL_ERR_INVALID;
+    int rc = cudil_verify(mode, ret, sm, sm_pitch, sb, sm + sb, sm_pitch, ml, pk, d_verify_pool, verify_pitch, batch,
+                          stream);
+    if (rc) return rc;
+    // the messages are released only for valid signatures: wait for the results
+    if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+        return cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
+    *mlen = ml;
+    for (size_t i = 0; i < batch && ml; ++i) {
+        if (ret[i] == 0)
+            std::memmove(m + i * m_pitch, sm + i * sm_pitch + sb, ml);
+        else
+            std::memset(m + i * m_pitch, 0, ml);
+    }
+    return CUDIL_OK;
 }
 
 int cudil_verify_dev(int mode, int *d_ret, const uint8_t *d_sig, size_t sig_pitch, size_t siglen, const uint8_t *d_m,

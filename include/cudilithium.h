@@ -115,6 +115,21 @@ int cudil_sign_dev_randomized(int mode, uint8_t *d_sig, size_t sig_pitch, const 
                               size_t temp_pool_pitch, cudil_task_lut *lut, size_t exec_threshold, size_t batch_size,
                               void *stream);
 
+/* Signed-message format of NIST-style callers (extends the reference, which has only detached
+ * signatures): sm row i = sig_i || m_i, smlen = sig_bytes + mlen.
+ * cudil_crypto_sign: host buffers as cudil_sign (m may lie inside sm; rows of sm are sm_pitch
+ *   apart and at least sig_bytes + mlen long).  Synchronizes `stream` once per rejection round.
+ * cudil_crypto_sign_open: verifies every row of smlen bytes; ret[i] = 0 and m row i = the message
+ *   if valid, else ret[i] = -1 and m row i zeroed; *mlen = smlen - sig_bytes (smlen < sig_bytes:
+ *   every ret[i] = -1, *mlen = 0).  Synchronizes `stream` before releasing the messages. */
+int cudil_crypto_sign(int mode, uint8_t *sm, size_t sm_pitch, size_t *smlen, const uint8_t *m, size_t m_pitch,
+                      size_t mlen, const uint8_t *sk, uint8_t *d_sign_pool, size_t sign_pool_pitch,
+                      uint8_t *d_temp_pool, size_t temp_pool_pitch, cudil_task_lut *lut, size_t exec_threshold,
+                      size_t batch_size, void *stream);
+int cudil_crypto_sign_open(int mode, uint8_t *m, size_t m_pitch, size_t *mlen, int *ret, const uint8_t *sm,
+                           size_t sm_pitch, size_t smlen, const uint8_t *pk, uint8_t *d_verify_pool,
+                           size_t verify_pool_pitch, size_t batch_size, void *stream);
+
 /* Batched well-formedness checks, a parse step of their own (extends the reference, whose hint
  * checks run inside verification, src/verify.cu:51-93).  All pointers are device memory; results
  * are asynchronous on `stream`.
