@@ -39,20 +39,32 @@ __global__ void __launch_bounds__(256) k_alu_peak(uint32_t *out, int iters) {
     out[blockIdx.x * blockDim.x + threadIdx.x] = r;
 }
 
-// One 16-thread group per polynomial: out = invNTT(NTT(a) o b).
+// out = invNTT(NTT(a) o b) for npolys polynomial pairs.  A grid of a few blocks per SM walks the
+// batch: each 16-thread group takes every total_groups-th polynomial, and while it transforms one it
+// already has the loads of the next a (issued before the inverse transform) and of the current b
+// (issued before the forward transform) in flight, so HBM latency overlaps the arithmetic.
 __global__ void __launch_bounds__(kBlock) k_ntt_mul(const int32_t *a, const int32_t *b, int32_t *out, long long npolys) {
     __shared__ int32_t sm[kGroupsPerBlock * NTT_SMEM_WORDS];
-    const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const long long groups = (long long)gridDim.x * (blockDim.x >> 4);
+    long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
     if (p >= npolys) return;
     Group g = make_group(sm, threadIdx.x >> 4);
     int32_t x[16], y[16];
     load16_strided(x, a + p * N, g.t);
-    ntt16(x, g.sm, g.gmask, g.t);
-    load16_contig(y, b + p * N + 16 * g.t);
+#pragma unroll 1
+    for (; p < npolys; p += groups) {
+        load16_contig(y, b + p * N + 16 * g.t);
+        ntt16(x, g.sm, g.gmask, g.t);
 #pragma unroll
-    for (int m = 0; m < 16; ++m) x[m] = montmul(x[m], y[m]);
-    intt16(x, g.sm, g.gmask, g.t);
-    store16_strided(out + p * N, x, g.t);
+        for (int m = 0; m < 16; ++m) x[m] = montmul(x[m], y[m]);
+        const long long nx = p + groups;
+        int32_t xn[16];
+        if (nx < npolys) load16_strided(xn, a + nx * N, g.t);
+        intt16(x, g.sm, g.gmask, g.t);
+        store16_strided(out + p * N, x, g.t);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = xn[m];
+    }
 }
 }  // namespace cudil
 
@@ -333,8 +345,18 @@ int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t
     if (!d_a || !d_b || !d_out) return CUDIL_ERR_INVALID;
     const size_t threads = npolys * 16;
     cudaStream_t st = (cudaStream_t)stream;
-    CUDIL_LAUNCH(KID_NTT_MUL, st,
-                 k_ntt_mul<<<(unsigned)((threads + kBlock - 1) / kBlock), kBlock, 0, st>>>(d_a, d_b, d_out, (long long)npolys));
+    // a few resident blocks per SM, each group looping over its share of the batch
+    static int blocks = 0;
+    if (!blocks) {
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ntt_mul, kBlock, 0) != cudaSuccess || per_sm < 1)
+            return cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
+        blocks = sms * per_sm;
+    }
+    const size_t need = (threads + kBlock - 1) / kBlock;
+    const unsigned grid = (unsigned)(need < (size_t)blocks ? need : (size_t)blocks);
+    CUDIL_LAUNCH(KID_NTT_MUL, st, k_ntt_mul<<<grid, kBlock, 0, st>>>(d_a, d_b, d_out, (long long)npolys));
     return cudaGetLastError() == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
 }
 
