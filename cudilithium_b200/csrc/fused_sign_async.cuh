@@ -45,7 +45,6 @@ struct AsyncSignSmem {
 };
 
 constexpr unsigned kAsyncIdleLimit = 1u << 21;  // idle polls (x ~0.3 us) before a block gives up
-constexpr int kKeccakSubpartition = 0;          // warps with warp % 4 == this prefer Keccak jobs
 
 template <int MODE, int THREADS, int NS>
 __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS) k_fused_sign_async(FusedSignArgs arg) {
@@ -55,7 +54,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
     constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA;
     constexpr int MS = 32 / L;  // slots per ExpandMask job
     static_assert(NS % 32 == 0 && NS >= 64, "slot count");
-    enum { CT_PEND = 0, CT_LOCK, CT_ERR, CT_SCAN, CT_INTT, CT_JOBS };
+    enum { CT_PEND = 0, CT_LOCK, CT_ERR, CT_SCAN, CT_INTT, CT_JOBS, CT_PREF };
     extern __shared__ __align__(16) uint8_t as_smem[];
     unsigned *s_item = reinterpret_cast<unsigned *>(as_smem);
     unsigned *s_nonce = s_item + NS;
@@ -562,27 +561,29 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
                 no_claim_pend = pend;
             }
         }
-        // job choice (warp-uniform inputs).  Warps of one SM sub-partition (warp % 4) prefer one
-        // kind of job -- Keccak on sub-partition 0, NTT on the others -- so each sub-partition's
-        // instruction cache holds mostly one kind of code; either kind falls back to the other
-        // when it has nothing to do.  Within a kind: finish attempts first, full Keccak batches
-        // before partial ones.
+        // job choice (warp-uniform inputs).  The block keeps one preferred job type, so that at
+        // any time most warps run the same code (a small instruction working set, as in a phased
+        // kernel) without ever waiting for each other: a warp takes the preferred type while it has
+        // a full job's worth of ready slots; otherwise it moves the preference to the type with the
+        // most ready work (finishing attempts first on ties) and takes that.
         int job = 0;  // 1 reject, 2 challenge, 3 w, 4 mask
-        const bool kec_role = (warp & 3) == kKeccakSubpartition;
-        if (kec_role) {
-            if (cC >= 32u) job = 2;
-            else if (cM >= (unsigned)MS) job = 4;
-            else if (cR) job = 1;
-            else if (cW) job = 3;
-            else if (cC) job = 2;
-            else if (cM) job = 4;
-        } else {
-            if (cR) job = 1;
-            else if (cW) job = 3;
-            else if (cC >= 32u) job = 2;
-            else if (cM >= (unsigned)MS) job = 4;
-            else if (cC) job = 2;
-            else if (cM) job = 4;
+        {
+            const unsigned pref = *reinterpret_cast<volatile unsigned *>(&s_ctl[CT_PREF]);
+            auto full = [&](int t) {
+                return t == 1 ? cR > 0u : t == 2 ? cC >= 32u : t == 3 ? cW > 0u : cM >= (unsigned)MS;
+            };
+            // ready work in warp jobs: one per reject / w slot, per 32 challenge or MS mask slots
+            const unsigned wR = cR, wC = (cC + 31u) / 32u, wW = cW, wM = (cM + MS - 1u) / (unsigned)MS;
+            if (pref >= 1u && pref <= 4u && full((int)pref)) {
+                job = (int)pref;
+            } else {
+                unsigned best = 0;
+                if (wR > best) { best = wR; job = 1; }
+                if (wW > best) { best = wW; job = 3; }
+                if (wC > best) { best = wC; job = 2; }
+                if (wM > best) { best = wM; job = 4; }
+                if (job && lane == 0) atomicExch(&s_ctl[CT_PREF], (unsigned)job);
+            }
         }
         const unsigned want_state = job == 1 ? AS_REJ : job == 2 ? AS_CH : job == 3 ? AS_W : AS_MASK;
         const int want = (job == 2) ? 32 : (job == 4 ? MS : 1);
