@@ -15,7 +15,7 @@
 //     same attempt (y_j / rows i / z_j / (r0_i, ct0_i) pairs), so both halves follow the same
 //     control flow and a rejection ends the job for the whole warp;
 //   * claiming (one warp at a time) turns FREE slots into MASK slots for the block's pending items,
-//     at most D attempts in flight per item, D = spec_slots / pending clamped to [1, 64];
+//     at most D attempts in flight per item, D = spec_slots / pending clamped to [1, 16];
 //   * an attempt whose nonce is above an already accepted nonce of its item is dropped at the next
 //     job boundary (it can no longer be the winner).
 // Every wait is bounded (idle polls, the per-item publication lock); running out sets an error bit
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
         unsigned D = 1;
         if (pend) {
             const unsigned t = target / pend;
-            D = t < 1u ? 1u : (t > 64u ? 64u : t);
+            D = t < 1u ? 1u : (t > 16u ? 16u : t);
         }
         unsigned filled = 0;  // grab[0, filled) hold an attempt (s_item set) or a failed placement
         const unsigned start = s_ctl[CT_SCAN];
