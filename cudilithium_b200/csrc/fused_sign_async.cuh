@@ -340,7 +340,37 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
         uint8_t *hs = slot + C::SL_SIG + PM::SIG_H;
         bool rejected = false;
         int n_intt = 0;
-        // z_j = y_j + invNTT(c s1_j), j = 2p + half
+        // Acceptance needs every check to pass, so the checks run most selective first: all
+        // r0_i = w0_i - invNTT(c s2_i) (kept in place of w0 for the hints), then the z_j, then
+        // ct0_i with the hints.  Pairs of polynomials: i / j = 2p + half (K even).
+#pragma unroll 1
+        for (int i0 = 0; i0 < K && !rejected; i0 += 2) {
+            const int i = i0 + half;
+            int32_t x[16], r0[16];
+            {
+                int32_t sv[16];
+                load16_contig(sv, s2 + (size_t)i * N + 16 * g.t);
+#pragma unroll
+                for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], sv[m]);
+            }
+            // w0 (thread-major) in flight during the transform
+            int32_t *w0t = reinterpret_cast<int32_t *>(slot + C::SL_W0 + (size_t)i * C::POLY) + 16 * g.t;
+            load16_contig(r0, w0t);
+            intt16_ool(x, g.sm, g.gmask, g.t);
+            bool bad = false;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                r0[m] = reduce32(r0[m] - x[m]);
+                bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
+            }
+            n_intt += 1;
+            if (__ballot_sync(FULL, bad)) {
+                rejected = true;
+                break;
+            }
+            store16_contig(w0t, r0);
+        }
+        // z_j = y_j + invNTT(c s1_j)
 #pragma unroll 1
         for (int j0 = 0; j0 < L && !rejected; j0 += 2) {
             const int j = j0 + half;
@@ -381,41 +411,23 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
                     reinterpret_cast<uint32_t *>(slot + C::SL_SIG + PM::SIG_Z + (size_t)j * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
             }
         }
-        // r0_i = w0_i - invNTT(c s2_i), ct0_i = invNTT(c t0_i), hints; i = 2p + half (K even)
+        // ct0_i = invNTT(c t0_i) and the hints of poly i
         int cnt = 0;
 #pragma unroll 1
         for (int i0 = 0; i0 < K && !rejected; i0 += 2) {
             const int i = i0 + half;
             int32_t x[16], r0[16];
             {
-                int32_t sv[16];
-                load16_contig(sv, s2 + (size_t)i * N + 16 * g.t);
-#pragma unroll
-                for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], sv[m]);
-            }
-            // w0 (thread-major) in flight during the transform
-            load16_contig(r0, reinterpret_cast<const int32_t *>(slot + C::SL_W0 + (size_t)i * C::POLY) + 16 * g.t);
-            intt16_ool(x, g.sm, g.gmask, g.t);
-            bool bad = false;
-#pragma unroll
-            for (int m = 0; m < 16; ++m) {
-                r0[m] = reduce32(r0[m] - x[m]);
-                bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
-            }
-            n_intt += 1;
-            if (__ballot_sync(FULL, bad)) {
-                rejected = true;
-                break;
-            }
-            {
                 int32_t tv[16];
                 load16_contig(tv, t0 + (size_t)i * N + 16 * g.t);
 #pragma unroll
                 for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], tv[m]);
             }
+            load16_contig(r0, reinterpret_cast<const int32_t *>(slot + C::SL_W0 + (size_t)i * C::POLY) + 16 * g.t);
             const uint4 w1v = *reinterpret_cast<const uint4 *>(slot + C::SL_W1B + (size_t)i * 256 + 16 * g.t);
             intt16_ool(x, g.sm, g.gmask, g.t);
             n_intt += 1;
+            bool bad = false;
 #pragma unroll
             for (int m = 0; m < 16; ++m) {
                 x[m] = reduce32(x[m]);
