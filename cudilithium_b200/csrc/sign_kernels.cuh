@@ -308,25 +308,27 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
     challenge_strided(ch, masks, g.t);
     ntt16(ch, g.sm, g.gmask, g.t);
 
-    // polynomial steps in the reference's order: z_0..z_{L-1}, then (r0_i, ct0_i) for i < K; one
-    // inverse-NTT call site, the next step's operand is loaded while the current one transforms
+    // Acceptance needs every check to pass (src/sign.cu:1026-1144 checks z, then r0, then ct0);
+    // here the most selective runs first: steps r0_0..r0_{K-1} (r0 replaces w0 in the temp row,
+    // for the hints), z_0..z_{L-1}, then ct0_0..ct0_{K-1} with the hints.  One inverse-NTT call
+    // site; the next step's operand loads while the current one transforms.
     const int32_t *s1 = reinterpret_cast<const int32_t *>(srow + LY::sg_s1(mlen));
     const int32_t *s2 = reinterpret_cast<const int32_t *>(srow + LY::sg_s2(mlen));
     const int32_t *t0 = reinterpret_cast<const int32_t *>(srow + LY::sg_t0(mlen));
     auto operand = [&](int step) -> const int32_t * {
-        if (step < L) return s1 + (size_t)step * N;
-        const int i = (step - L) >> 1;
-        return ((((step - L) & 1) == 0) ? s2 : t0) + (size_t)i * N;
+        if (step < K) return s2 + (size_t)step * N;
+        if (step < K + L) return s1 + (size_t)(step - K) * N;
+        return t0 + (size_t)(step - K - L) * N;
     };
     uint8_t *hs = trow + LY::TP_SIG + PM::SIG_H;
     const int lane_off = threadIdx.x & 16;
     int cnt = 0;
-    int32_t r0[16], nx[16];
+    int32_t nx[16];
     load16_contig(nx, operand(0) + 16 * g.t);
 #pragma unroll 1
     for (int step = 0; step < L + 2 * K; ++step) {
-        const int i = (step - L) >> 1;
-        const bool is_z = step < L, is_r0 = !is_z && (((step - L) & 1) == 0);
+        const bool is_r0 = step < K, is_z = !is_r0 && step < K + L;
+        const int i = is_r0 ? step : step - K - L;
         int32_t x[16];
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], nx[m]);
@@ -334,8 +336,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
         intt16(x, g.sm, g.gmask, g.t);
         bool bad = false;
         if (is_z) {
+            const int j = step - K;
             int32_t y[16];
-            unpack_z_strided<MODE>(y, trow + LY::TP_Y + (size_t)step * PM::POLYZ_PACKED, g.t);
+            unpack_z_strided<MODE>(y, trow + LY::TP_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
 #pragma unroll
             for (int m = 0; m < 16; ++m) {
                 x[m] = reduce32(x[m] + y[m]);
@@ -348,15 +351,18 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
 #pragma unroll
             for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
             pack16_words<PM::Z_BITS>(
-                reinterpret_cast<uint32_t *>(trow + LY::TP_SIG + PM::SIG_Z + (size_t)step * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
+                reinterpret_cast<uint32_t *>(trow + LY::TP_SIG + PM::SIG_Z + (size_t)j * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
         } else if (is_r0) {
-            const int32_t *w0 = reinterpret_cast<const int32_t *>(trow + LY::TP_W0) + (size_t)i * N;
+            int32_t *w0 = reinterpret_cast<int32_t *>(trow + LY::TP_W0) + (size_t)i * N;
+            int32_t r0[16];
 #pragma unroll
             for (int m = 0; m < 16; ++m) {
                 r0[m] = reduce32(w0[g.t + 16 * m] - x[m]);
                 bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
             }
             if (group_any(g, bad)) return;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) w0[g.t + 16 * m] = r0[m];
         } else {
 #pragma unroll
             for (int m = 0; m < 16; ++m) {
@@ -364,11 +370,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
                 bad |= exceeds(x[m], PM::GAMMA2);
             }
             if (group_any(g, bad)) return;
+            const int32_t *r0 = reinterpret_cast<const int32_t *>(trow + LY::TP_W0) + (size_t)i * N;
             const uint8_t *w1p = trow + LY::TP_W1P + (size_t)i * PM::POLYW1_PACKED;
 #pragma unroll
             for (int m = 0; m < 16; ++m) {
                 const int32_t w1 = (int32_t)get_bits(w1p, (g.t + 16 * m) * PM::W1_BITS, PM::W1_BITS);
-                const unsigned h = make_hint<MODE>(r0[m] + x[m], w1);
+                const unsigned h = make_hint<MODE>(r0[g.t + 16 * m] + x[m], w1);
                 const unsigned bal = (__ballot_sync(g.gmask, h) >> lane_off) & 0xFFFFu;
                 if (h) {
                     const int idx = cnt + __popc(bal & ((1u << g.t) - 1u));
