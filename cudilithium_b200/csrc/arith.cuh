@@ -61,6 +61,53 @@ static_assert(kTwiddles.zeta[1] == 25847, "zeta table");
 static_assert(kTwiddles.zeta[2] == -2608894, "zeta table");
 static_assert(kTwiddles.zeta[255] == 1976782, "zeta table");
 
+// Precomputed-quotient (Shoup) twiddles for the butterflies of the signing / verification
+// transforms: the same zetas as true residues w = 1753^brv8(i) mod q (centred) with
+// w_q = floor(w * 2^32 / q).  shoup_mul(b, w, w_q) = b * w - q * floor(b * w_q / 2^32) is
+// congruent to b * w mod q and lies in (-q/2, 3q/2) for any 32-bit b -- one high multiply and two
+// low multiply-adds instead of montmul's two high multiplies, one low multiply and a subtraction.
+// The transforms built on it give the reference's residues (not its representatives), so they
+// serve every path whose outputs are reduced before use; key generation and the NTT microbench,
+// whose outputs are compared representative for representative, keep the Montgomery transforms.
+__host__ __device__ constexpr int32_t shoup_quot(int32_t w) {
+    const int64_t num = (int64_t)w * (int64_t)(1ll << 32);
+    int64_t qq = num / Q;
+    if (num < 0 && qq * Q != num) --qq;  // floor
+    return (int32_t)qq;
+}
+
+__host__ __device__ constexpr TwiddleTables make_shoup_twiddles() {
+    TwiddleTables t{};
+    for (int i = 0; i < N; ++i) {
+        uint64_t e = brv8((unsigned)i), r = 1, b = 1753;
+        while (e) {
+            if (e & 1) r = r * b % Q;
+            b = b * b % Q;
+            e >>= 1;
+        }
+        int32_t w = (int32_t)(r > (uint64_t)(Q - 1) / 2 ? (int64_t)r - Q : (int64_t)r);
+        if (i == 0) w = 0;
+        t.zeta[i] = w;
+        t.zeta_q[i] = shoup_quot(w);
+        t.izeta[i] = -w;
+        t.izeta_q[i] = shoup_quot(-w);
+    }
+    return t;
+}
+
+constexpr TwiddleTables kShoupTwiddles = make_shoup_twiddles();
+
+// every true twiddle times mont is the Montgomery-form twiddle (mod q)
+__host__ __device__ constexpr bool shoup_matches_montgomery() {
+    const int64_t mont = (int64_t)((1ull << 32) % Q);
+    for (int i = 1; i < N; ++i) {
+        const int64_t a = ((int64_t)kShoupTwiddles.zeta[i] * mont - (int64_t)kTwiddles.zeta[i]) % Q;
+        if (a != 0) return false;
+    }
+    return true;
+}
+static_assert(shoup_matches_montgomery(), "shoup table");
+
 // f = mont^2 / 256 (the reference's 41978) and its QINV product.
 constexpr int32_t F_INV = 41978;
 constexpr int32_t F_INV_Q = mul_qinv(41978);
@@ -78,6 +125,11 @@ __device__ __forceinline__ int32_t montmul(int32_t a, int32_t b) {
 // result is bit-identical to montmul(a, z) with one multiplication fewer.
 __device__ __forceinline__ int32_t montmul_pre(int32_t a, int32_t z, int32_t zq) {
     return __mulhi(a, z) - __mulhi(a * zq, Q);
+}
+
+__device__ __forceinline__ int32_t shoup_mul(int32_t b, int32_t w, int32_t wq) {
+    const int32_t t = __mulhi(b, wq);
+    return (int32_t)((uint32_t)b * (uint32_t)w - (uint32_t)t * (uint32_t)Q);
 }
 
 __device__ __forceinline__ int32_t reduce32(int32_t a) {

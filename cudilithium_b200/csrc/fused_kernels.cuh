@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(kBlock) k_cache_sk(const uint8_t *sk, uint8_t 
         }
         dst = C::SK_T0 + (size_t)(p - L - K) * C::POLY;
     }
-    ntt16(x, g.sm, g.gmask, g.t);
+    ntt16s(x, g.sm, g.gmask, g.t);
     store16_contig(reinterpret_cast<int32_t *>(row + dst) + 16 * g.t, x);
 }
 
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kBlock) k_cache_pk_t1(const uint8_t *pk, uint8
         const uint32_t v = ((uint32_t)t1p[byte] | ((uint32_t)t1p[byte + 1] << 8)) >> sh;  // sh + 10 <= 16
         x[m] = (int32_t)((v & 0x3FFu) << D);
     }
-    ntt16(x, g.sm, g.gmask, g.t);
+    ntt16s(x, g.sm, g.gmask, g.t);
     store16_contig(reinterpret_cast<int32_t *>(rows + (size_t)it * pitch + C::PK_T1 + (size_t)i * C::POLY) + 16 * g.t, x);
 }
 
@@ -815,7 +815,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
                         x[m] = PM::GAMMA1 - (int32_t)(v & ((1u << PM::Z_BITS) - 1u));
                         zbad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
                     }
-                    ntt16(x, g.sm, g.gmask, g.t);
+                    ntt16s(x, g.sm, g.gmask, g.t);
                     store16_smem(zh + j * N, x, g.t);
                 }
                 if (group_any(g, zbad) && g.t == 0) reinterpret_cast<int *>(slot + C::VS_STATUS)[0] |= 2;
@@ -832,7 +832,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
                     }
                     int32_t x[16];
                     challenge_strided(x, masks, g.t);
-                    ntt16(x, g.sm, g.gmask, g.t);
+                    ntt16s(x, g.sm, g.gmask, g.t);
                     store16_smem(zh + L * N, x, g.t);
                 }
                 __syncwarp(g.gmask);
@@ -863,7 +863,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
                     load16_contig(tv, reinterpret_cast<const int32_t *>(row + C::PK_T1) + (size_t)i * N + 16 * g.t);
 #pragma unroll
                     for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m] - montmul(cv[m], tv[m]));
-                    intt16(acc, g.sm, g.gmask, g.t);
+                    intt16s(acc, g.sm, g.gmask, g.t);
                     int32_t w1[16];
 #pragma unroll
                     for (int m = 0; m < 16; ++m) {

@@ -31,44 +31,60 @@ struct GroupTwiddles {
     int2 inv[16][16];  // levels len 1,2,4,8 of the inverse transform (negated zetas)
 };
 
-__host__ __device__ constexpr GroupTwiddles make_group_twiddles() {
+__host__ __device__ constexpr GroupTwiddles make_group_twiddles(const TwiddleTables &tw) {
     GroupTwiddles g{};
     for (int t = 0; t < 16; ++t) {
         int n = 0;
         // forward: len 8: zeta[16+t]; len 4: zeta[32+2t+m]; len 2: zeta[64+4t+m]; len 1: zeta[128+8t+m]
-        g.fwd[t][n++] = int2{kTwiddles.zeta[16 + t], kTwiddles.zeta_q[16 + t]};
-        for (int m = 0; m < 2; ++m) g.fwd[t][n++] = int2{kTwiddles.zeta[32 + 2 * t + m], kTwiddles.zeta_q[32 + 2 * t + m]};
-        for (int m = 0; m < 4; ++m) g.fwd[t][n++] = int2{kTwiddles.zeta[64 + 4 * t + m], kTwiddles.zeta_q[64 + 4 * t + m]};
-        for (int m = 0; m < 8; ++m) g.fwd[t][n++] = int2{kTwiddles.zeta[128 + 8 * t + m], kTwiddles.zeta_q[128 + 8 * t + m]};
+        g.fwd[t][n++] = int2{tw.zeta[16 + t], tw.zeta_q[16 + t]};
+        for (int m = 0; m < 2; ++m) g.fwd[t][n++] = int2{tw.zeta[32 + 2 * t + m], tw.zeta_q[32 + 2 * t + m]};
+        for (int m = 0; m < 4; ++m) g.fwd[t][n++] = int2{tw.zeta[64 + 4 * t + m], tw.zeta_q[64 + 4 * t + m]};
+        for (int m = 0; m < 8; ++m) g.fwd[t][n++] = int2{tw.zeta[128 + 8 * t + m], tw.zeta_q[128 + 8 * t + m]};
         g.fwd[t][15] = int2{0, 0};
         n = 0;
         // inverse: len 1: -zeta[255-8t-m]; len 2: -zeta[127-4t-m]; len 4: -zeta[63-2t-m]; len 8: -zeta[31-t]
-        for (int m = 0; m < 8; ++m) g.inv[t][n++] = int2{kTwiddles.izeta[255 - 8 * t - m], kTwiddles.izeta_q[255 - 8 * t - m]};
-        for (int m = 0; m < 4; ++m) g.inv[t][n++] = int2{kTwiddles.izeta[127 - 4 * t - m], kTwiddles.izeta_q[127 - 4 * t - m]};
-        for (int m = 0; m < 2; ++m) g.inv[t][n++] = int2{kTwiddles.izeta[63 - 2 * t - m], kTwiddles.izeta_q[63 - 2 * t - m]};
-        g.inv[t][n++] = int2{kTwiddles.izeta[31 - t], kTwiddles.izeta_q[31 - t]};
+        for (int m = 0; m < 8; ++m) g.inv[t][n++] = int2{tw.izeta[255 - 8 * t - m], tw.izeta_q[255 - 8 * t - m]};
+        for (int m = 0; m < 4; ++m) g.inv[t][n++] = int2{tw.izeta[127 - 4 * t - m], tw.izeta_q[127 - 4 * t - m]};
+        for (int m = 0; m < 2; ++m) g.inv[t][n++] = int2{tw.izeta[63 - 2 * t - m], tw.izeta_q[63 - 2 * t - m]};
+        g.inv[t][n++] = int2{tw.izeta[31 - t], tw.izeta_q[31 - t]};
         g.inv[t][15] = int2{0, 0};
     }
     return g;
 }
 
-static __device__ const GroupTwiddles g_group_tw = make_group_twiddles();
+static __device__ const GroupTwiddles g_group_tw = make_group_twiddles(kTwiddles);
+static __device__ const GroupTwiddles g_group_tw_s = make_group_twiddles(kShoupTwiddles);
 // Uniform twiddles (same for all threads of a group): zeta[1..15] and -zeta[1..15].
 static __constant__ TwiddleTables c_tw = make_twiddles();
+static __constant__ TwiddleTables c_tw_s = make_shoup_twiddles();
 
 // Shared-memory words per group for the transpose (16 rows of 17).
 constexpr int NTT_SMEM_WORDS = 16 * 17;
 
+// Butterfly multiply: S = false Montgomery (twiddles in Montgomery form, the reference's exact
+// representatives), S = true precomputed quotient (true twiddles, same residues).
+template <bool S>
+__device__ __forceinline__ int32_t bfly_mul(int32_t b, int32_t z, int32_t zq) {
+    return S ? shoup_mul(b, z, zq) : montmul_pre(b, z, zq);
+}
+
+template <bool S = false>
 __device__ __forceinline__ void ct_bfly(int32_t &a, int32_t &b, int32_t z, int32_t zq) {
-    int32_t t = montmul_pre(b, z, zq);
+    int32_t t = bfly_mul<S>(b, z, zq);
     b = a - t;
     a = a + t;
 }
 
+template <bool S = false>
 __device__ __forceinline__ void gs_bfly(int32_t &a, int32_t &b, int32_t z, int32_t zq) {
     int32_t t = a;
     a = t + b;
-    b = montmul_pre(t - b, z, zq);
+    b = bfly_mul<S>(t - b, z, zq);
+}
+
+template <bool S>
+__device__ __forceinline__ const TwiddleTables &utw() {
+    return S ? c_tw_s : c_tw;
 }
 
 __device__ __forceinline__ void load_tw16(int2 (&tw)[16], const int2 *src) {
@@ -82,21 +98,22 @@ __device__ __forceinline__ void load_tw16(int2 (&tw)[16], const int2 *src) {
 }
 
 // Forward NTT; sm = this group's NTT_SMEM_WORDS-word region, gmask = this group's lanes.
-__device__ __forceinline__ void ntt16(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
+template <bool S>
+__device__ __forceinline__ void ntt16_t(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
     // len 128: (i, i+8), zeta[1]
 #pragma unroll
-    for (int i = 0; i < 8; ++i) ct_bfly(x[i], x[i + 8], c_tw.zeta[1], c_tw.zeta_q[1]);
+    for (int i = 0; i < 8; ++i) ct_bfly<S>(x[i], x[i + 8], utw<S>().zeta[1], utw<S>().zeta_q[1]);
     // len 64: (i, i+4), zeta[2 + (i>>3)]
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-        if (!(i & 4)) ct_bfly(x[i], x[i + 4], c_tw.zeta[2 + (i >> 3)], c_tw.zeta_q[2 + (i >> 3)]);
+        if (!(i & 4)) ct_bfly<S>(x[i], x[i + 4], utw<S>().zeta[2 + (i >> 3)], utw<S>().zeta_q[2 + (i >> 3)]);
     // len 32: (i, i+2), zeta[4 + (i>>2)]
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-        if (!(i & 2)) ct_bfly(x[i], x[i + 2], c_tw.zeta[4 + (i >> 2)], c_tw.zeta_q[4 + (i >> 2)]);
+        if (!(i & 2)) ct_bfly<S>(x[i], x[i + 2], utw<S>().zeta[4 + (i >> 2)], utw<S>().zeta_q[4 + (i >> 2)]);
     // len 16: (i, i+1), zeta[8 + (i>>1)]
 #pragma unroll
-    for (int i = 0; i < 16; i += 2) ct_bfly(x[i], x[i + 1], c_tw.zeta[8 + (i >> 1)], c_tw.zeta_q[8 + (i >> 1)]);
+    for (int i = 0; i < 16; i += 2) ct_bfly<S>(x[i], x[i + 1], utw<S>().zeta[8 + (i >> 1)], utw<S>().zeta_q[8 + (i >> 1)]);
 
     // transpose: a[j] lives at sm[j + (j >> 4)]
 #pragma unroll
@@ -107,41 +124,42 @@ __device__ __forceinline__ void ntt16(int32_t (&x)[16], int32_t *sm, unsigned gm
     __syncwarp(gmask);
 
     int2 tw[16];
-    load_tw16(tw, g_group_tw.fwd[t]);
+    load_tw16(tw, (S ? g_group_tw_s : g_group_tw).fwd[t]);
     // len 8: (i, i+8), zeta[16+t]
 #pragma unroll
-    for (int i = 0; i < 8; ++i) ct_bfly(x[i], x[i + 8], tw[0].x, tw[0].y);
+    for (int i = 0; i < 8; ++i) ct_bfly<S>(x[i], x[i + 8], tw[0].x, tw[0].y);
     // len 4: zeta[32 + 2t + (i>>3)]
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-        if (!(i & 4)) ct_bfly(x[i], x[i + 4], tw[1 + (i >> 3)].x, tw[1 + (i >> 3)].y);
+        if (!(i & 4)) ct_bfly<S>(x[i], x[i + 4], tw[1 + (i >> 3)].x, tw[1 + (i >> 3)].y);
     // len 2: zeta[64 + 4t + (i>>2)]
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-        if (!(i & 2)) ct_bfly(x[i], x[i + 2], tw[3 + (i >> 2)].x, tw[3 + (i >> 2)].y);
+        if (!(i & 2)) ct_bfly<S>(x[i], x[i + 2], tw[3 + (i >> 2)].x, tw[3 + (i >> 2)].y);
     // len 1: zeta[128 + 8t + (i>>1)]
 #pragma unroll
-    for (int i = 0; i < 16; i += 2) ct_bfly(x[i], x[i + 1], tw[7 + (i >> 1)].x, tw[7 + (i >> 1)].y);
+    for (int i = 0; i < 16; i += 2) ct_bfly<S>(x[i], x[i + 1], tw[7 + (i >> 1)].x, tw[7 + (i >> 1)].y);
 }
 
 // Inverse NTT including the final multiplication by f (invntt_tomont).
-__device__ __forceinline__ void intt16(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
+template <bool S>
+__device__ __forceinline__ void intt16_t(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
     int2 tw[16];
-    load_tw16(tw, g_group_tw.inv[t]);
+    load_tw16(tw, (S ? g_group_tw_s : g_group_tw).inv[t]);
     // len 1: block 8t + (i>>1): -zeta[255 - 8t - (i>>1)]
 #pragma unroll
-    for (int i = 0; i < 16; i += 2) gs_bfly(x[i], x[i + 1], tw[i >> 1].x, tw[i >> 1].y);
+    for (int i = 0; i < 16; i += 2) gs_bfly<S>(x[i], x[i + 1], tw[i >> 1].x, tw[i >> 1].y);
     // len 2: -zeta[127 - 4t - (i>>2)]
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-        if (!(i & 2)) gs_bfly(x[i], x[i + 2], tw[8 + (i >> 2)].x, tw[8 + (i >> 2)].y);
+        if (!(i & 2)) gs_bfly<S>(x[i], x[i + 2], tw[8 + (i >> 2)].x, tw[8 + (i >> 2)].y);
     // len 4: -zeta[63 - 2t - (i>>3)]
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-        if (!(i & 4)) gs_bfly(x[i], x[i + 4], tw[12 + (i >> 3)].x, tw[12 + (i >> 3)].y);
+        if (!(i & 4)) gs_bfly<S>(x[i], x[i + 4], tw[12 + (i >> 3)].x, tw[12 + (i >> 3)].y);
     // len 8: -zeta[31 - t]
 #pragma unroll
-    for (int i = 0; i < 8; ++i) gs_bfly(x[i], x[i + 8], tw[14].x, tw[14].y);
+    for (int i = 0; i < 8; ++i) gs_bfly<S>(x[i], x[i + 8], tw[14].x, tw[14].y);
 
 #pragma unroll
     for (int i = 0; i < 16; ++i) sm[17 * t + i] = x[i];
@@ -152,21 +170,30 @@ __device__ __forceinline__ void intt16(int32_t (&x)[16], int32_t *sm, unsigned g
 
     // len 16: (i, i+1): -zeta[15 - (i>>1)]
 #pragma unroll
-    for (int i = 0; i < 16; i += 2) gs_bfly(x[i], x[i + 1], c_tw.izeta[15 - (i >> 1)], c_tw.izeta_q[15 - (i >> 1)]);
+    for (int i = 0; i < 16; i += 2) gs_bfly<S>(x[i], x[i + 1], utw<S>().izeta[15 - (i >> 1)], utw<S>().izeta_q[15 - (i >> 1)]);
     // len 32: -zeta[7 - (i>>2)]
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-        if (!(i & 2)) gs_bfly(x[i], x[i + 2], c_tw.izeta[7 - (i >> 2)], c_tw.izeta_q[7 - (i >> 2)]);
+        if (!(i & 2)) gs_bfly<S>(x[i], x[i + 2], utw<S>().izeta[7 - (i >> 2)], utw<S>().izeta_q[7 - (i >> 2)]);
     // len 64: -zeta[3 - (i>>3)]
 #pragma unroll
     for (int i = 0; i < 16; ++i)
-        if (!(i & 4)) gs_bfly(x[i], x[i + 4], c_tw.izeta[3 - (i >> 3)], c_tw.izeta_q[3 - (i >> 3)]);
+        if (!(i & 4)) gs_bfly<S>(x[i], x[i + 4], utw<S>().izeta[3 - (i >> 3)], utw<S>().izeta_q[3 - (i >> 3)]);
     // len 128: -zeta[1]
 #pragma unroll
-    for (int i = 0; i < 8; ++i) gs_bfly(x[i], x[i + 8], c_tw.izeta[1], c_tw.izeta_q[1]);
+    for (int i = 0; i < 8; ++i) gs_bfly<S>(x[i], x[i + 8], utw<S>().izeta[1], utw<S>().izeta_q[1]);
 #pragma unroll
     for (int i = 0; i < 16; ++i) x[i] = montmul_pre(x[i], F_INV, F_INV_Q);
 }
+
+// Montgomery transforms: the reference's exact output representatives (key generation, the NTT
+// microbench).
+__device__ __forceinline__ void ntt16(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) { ntt16_t<false>(x, sm, gmask, t); }
+__device__ __forceinline__ void intt16(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) { intt16_t<false>(x, sm, gmask, t); }
+// Precomputed-quotient transforms: the same residues, cheaper butterflies (signing, verification,
+// the engine's key caches -- every consumer reduces the outputs before use).
+__device__ __forceinline__ void ntt16s(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) { ntt16_t<true>(x, sm, gmask, t); }
+__device__ __forceinline__ void intt16s(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) { intt16_t<true>(x, sm, gmask, t); }
 
 // Out-of-line forms of the two transforms for large kernels that call them from many places: one
 // copy of each transform instead of one per call site keeps the instruction working set small.
@@ -176,12 +203,12 @@ struct Coef16 {
 };
 
 static __device__ __noinline__ Coef16 ntt16_call(Coef16 x, int32_t *sm, unsigned gmask, int t) {
-    ntt16(x.v, sm, gmask, t);
+    ntt16s(x.v, sm, gmask, t);
     return x;
 }
 
 static __device__ __noinline__ Coef16 intt16_call(Coef16 x, int32_t *sm, unsigned gmask, int t) {
-    intt16(x.v, sm, gmask, t);
+    intt16s(x.v, sm, gmask, t);
     return x;
 }
 

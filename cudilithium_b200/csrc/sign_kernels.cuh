@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_unpack_ntt(uint8_t *pool, size_
         for (int i = 0; i < 16; ++i) x[i] = (1 << (D - 1)) - (int32_t)get_bits(src, (g.t + 16 * i) * 13, 13);
         dst = LY::sg_t0(mlen) + (size_t)(p - L - K) * LY::POLY;
     }
-    ntt16(x, g.sm, g.gmask, g.t);
+    ntt16s(x, g.sm, g.gmask, g.t);
     store16_contig(reinterpret_cast<int32_t *>(row + dst) + 16 * g.t, x);
 }
 
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_compute_w(const uint8_t *sign_p
         if (e >= nexec) continue;
         int32_t x[16];
         unpack_z_strided<MODE>(x, temp_pool + (size_t)e * tp + LY::TP_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
-        ntt16(x, g.sm, g.gmask, g.t);
+        ntt16s(x, g.sm, g.gmask, g.t);
         store16_smem(&s_yhat[a][j][0], x, g.t);
     }
     __syncthreads();
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_compute_w(const uint8_t *sign_p
         }
 #pragma unroll
         for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m]);
-        intt16(acc, g.sm, g.gmask, g.t);
+        intt16s(acc, g.sm, g.gmask, g.t);
         uint8_t *trow = temp_pool + (size_t)e * tp;
         int32_t *w0 = reinterpret_cast<int32_t *>(trow + LY::TP_W0) + (size_t)i * N;
         int32_t w1[16];
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
     }
     int32_t ch[16];
     challenge_strided(ch, masks, g.t);
-    ntt16(ch, g.sm, g.gmask, g.t);
+    ntt16s(ch, g.sm, g.gmask, g.t);
 
     // Acceptance needs every check to pass (src/sign.cu:1026-1144 checks z, then r0, then ct0);
     // here the most selective runs first: steps r0_0..r0_{K-1} (r0 replaces w0 in the temp row,
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], nx[m]);
         if (step + 1 < L + 2 * K) load16_contig(nx, operand(step + 1) + 16 * g.t);
-        intt16(x, g.sm, g.gmask, g.t);
+        intt16s(x, g.sm, g.gmask, g.t);
         bool bad = false;
         if (is_z) {
             const int j = step - K;

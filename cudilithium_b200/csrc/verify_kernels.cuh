@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kBlock) k_verify_w(uint8_t *pool, size_t pitch
             }
             challenge_strided(x, masks, g.t);
         }
-        ntt16(x, g.sm, g.gmask, g.t);
+        ntt16s(x, g.sm, g.gmask, g.t);
         store16_smem(&s_hat[a][j][0], x, g.t);
     }
     __syncthreads();
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kBlock) k_verify_w(uint8_t *pool, size_t pitch
         const uint8_t *t1p = row + LY::VF_PK + SEEDBYTES + (size_t)i * POLYT1_PACKED;
 #pragma unroll
         for (int m = 0; m < 16; ++m) t1[m] = (int32_t)(get_bits(t1p, (g.t + 16 * m) * 10, 10) << D);
-        ntt16(t1, g.sm, g.gmask, g.t);
+        ntt16s(t1, g.sm, g.gmask, g.t);
         const int32_t *mat = reinterpret_cast<const int32_t *>(row + LY::vf_mat(mlen)) + (size_t)i * L * N;
         int32_t acc[16];
 #pragma unroll
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(kBlock) k_verify_w(uint8_t *pool, size_t pitch
         load16_smem(cv, &s_hat[a][L][0], g.t);
 #pragma unroll
         for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m] - montmul(cv[m], t1[m]));
-        intt16(acc, g.sm, g.gmask, g.t);
+        intt16s(acc, g.sm, g.gmask, g.t);
         int32_t w1[16];
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
