@@ -2,10 +2,14 @@
 // threads (16 coefficients each, two groups per warp).
 //
 // Arithmetic: the same Cooley-Tukey (forward) and Gentleman-Sande (inverse) butterfly network
-// as the reference (src/ntt.cu:58-207, include/ntt.cuh:74-306): every butterfly is
-// a +/- montmul(zeta, b) with the same zeta, and the inverse ends with a multiplication of
-// every coefficient by f = 41978 (src/ntt.cu:201-205), so outputs are bit-identical to the
-// reference's radix-8 kernels and to the CPU oracle.
+// as the reference (src/ntt.cu:58-207, include/ntt.cuh:74-306), and the inverse ends with a
+// Montgomery multiplication of every coefficient by f = 41978 (src/ntt.cu:201-205).  Two forms:
+//   ntt16 / intt16   every butterfly is a +/- montmul(zeta, b) with the reference's Montgomery
+//                    zetas, so outputs are bit-identical to the reference's radix-8 kernels and to
+//                    the CPU oracle (key generation, the NTT microbench);
+//   ntt16s / intt16s the butterflies multiply by the true zetas with precomputed quotients
+//                    (shoup_mul): the same residues mod q in other representatives, for the
+//                    signing and verification paths, which reduce every output before use.
 //
 // Layout (radix-16, one shared-memory transpose per transform instead of two):
 //   forward: in  x[i] = a[t + 16 i]  -> levels len 128..16 in registers
