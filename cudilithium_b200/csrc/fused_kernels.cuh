@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
     using PM = P<MODE>;
     using C = Cache<MODE>;
     constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA, A = THREADS, G = THREADS / 16;
-    enum { CT_PEND = 0, CT_KJOB, CT_NJOB, CT_NA0, CT_NA1, CT_EXIT };
+    enum { CT_PEND = 0, CT_KJOB, CT_NJOB, CT_NA0, CT_NA1 };
     extern __shared__ __align__(16) uint8_t fs_smem[];
     unsigned *s_item = reinterpret_cast<unsigned *>(fs_smem);   // [2][A]
     unsigned *s_nonce = s_item + 2 * A;                          // [2][A]

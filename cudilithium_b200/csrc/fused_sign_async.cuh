@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
     constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA;
     constexpr int MS = 32 / L;  // slots per ExpandMask job
     static_assert(NS % 32 == 0 && NS >= 64, "slot count");
-    enum { CT_PEND = 0, CT_LOCK, CT_ERR, CT_SCAN, CT_INTT, CT_JOBS, CT_PREF };
+    enum { CT_PEND = 0, CT_LOCK, CT_ERR, CT_SCAN, CT_INTT, CT_PREF };
     extern __shared__ __align__(16) uint8_t as_smem[];
     unsigned *s_item = reinterpret_cast<unsigned *>(as_smem);
     unsigned *s_nonce = s_item + NS;

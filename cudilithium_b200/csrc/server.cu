@@ -105,10 +105,9 @@ struct Slot {
         const size_t sigb = p.sig_bytes;
         const auto c0 = Clock::now();
         // stage messages (fused: packed at 8-byte aligned offsets; plain: rows of cfg->max_mlen)
-        size_t pos = 0, maxl = 0;
+        size_t pos = 0;
         for (size_t i = 0; i < n; ++i) {
             const cudil_request &r = tr->reqs[batch[i]];
-            maxl = std::max<size_t>(maxl, r.mlen);
             if (cfg->path == 0) {
                 off[i] = pos;
                 std::memcpy(h_msgs + pos, tr->msgs + r.msg_off, r.mlen);
