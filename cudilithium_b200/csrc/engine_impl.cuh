@@ -35,6 +35,8 @@ struct EngineBase {
     unsigned long long *d_off = nullptr;
     uint8_t *h_stage = nullptr;     // [FusedQueue | key | mlen | order | off]
     FusedQueue *h_status = nullptr; // D2H copy of the queue after a batch
+    cudaEvent_t stage_ev = nullptr; // recorded after a batch's metadata upload from h_stage
+    bool stage_pending = false;
     uint8_t *scratch = nullptr;
     size_t scratch_bytes = 0;
     int sign_grid = 0, verify_grid = 0, prehash_grid = 0;
@@ -151,6 +153,7 @@ struct EngineImpl : EngineBase {
             cudaMallocHost(&h_status, sizeof(FusedQueue)) != cudaSuccess)
             return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
         std::memset(h_status, 0, sizeof(FusedQueue));
+        CUDIL_CK(cudaEventCreateWithFlags(&stage_ev, cudaEventDisableTiming));
         CUDIL_CK(cudaMemset(q, 0, sizeof(FusedQueue)));
         return CUDIL_OK;
     }
@@ -175,6 +178,7 @@ struct EngineImpl : EngineBase {
         cudaFree(scratch);
         if (h_stage) cudaFreeHost(h_stage);
         if (h_status) cudaFreeHost(h_status);
+        if (stage_ev) cudaEventDestroy(stage_ev);
     }
 
     // ------------------------------------------------------------ key caches
@@ -227,8 +231,10 @@ struct EngineImpl : EngineBase {
     // ------------------------------------------------------------ metadata upload
     int upload_meta(const unsigned long long *off, const unsigned *mlen, const unsigned *key, size_t n, size_t nkeys,
                     size_t msgs_bytes, bool longest_first, cudaStream_t st) {
-        // the previous batch's upload from the staging buffer must have completed
-        CUDIL_CK(cudaStreamSynchronize(st));
+        // the previous batch's copies out of the staging buffer must have completed (only those:
+        // work the caller queued on the stream, such as input copies or cache builds, keeps
+        // running while this batch is prepared)
+        if (stage_pending) CUDIL_CK(cudaEventSynchronize(stage_ev));
         FusedQueue *hq = reinterpret_cast<FusedQueue *>(h_stage);
         std::memset(hq, 0, sizeof(FusedQueue));
         hq->n = (unsigned)n;
@@ -251,6 +257,8 @@ struct EngineImpl : EngineBase {
         CUDIL_CK(cudaMemcpyAsync(d_mlen, hm, n * sizeof(unsigned), cudaMemcpyHostToDevice, st));
         CUDIL_CK(cudaMemcpyAsync(d_order, ho, n * sizeof(unsigned), cudaMemcpyHostToDevice, st));
         CUDIL_CK(cudaMemcpyAsync(d_off, hoff, n * sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+        CUDIL_CK(cudaEventRecord(stage_ev, st));
+        stage_pending = true;
         return CUDIL_OK;
     }
 
