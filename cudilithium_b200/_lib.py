@@ -117,6 +117,7 @@ SIGNATURES = {
     "cudil_engine_destroy": (c_int, [c_void_p]),
     "cudil_engine_device_bytes": (c_size_t, [c_void_p]),
     "cudil_engine_set_secret_keys": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
+    "cudil_engine_update_secret_keys": (c_int, [c_void_p, c_void_p, c_size_t, c_size_t, c_void_p]),
     "cudil_engine_attach_keys": (c_int, [c_void_p, c_void_p]),
     "cudil_engine_set_public_keys": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
     "cudil_engine_sign": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_size_t,

@@ -85,6 +85,10 @@ int cudil_engine_set_secret_keys(cudil_engine *e, const uint8_t *d_sk, size_t nk
     CUDIL_ENGINE_DISPATCH(e, set_secret_keys(d_sk, nkeys, (cudaStream_t)stream));
 }
 
+int cudil_engine_update_secret_keys(cudil_engine *e, const uint8_t *d_sk, size_t first, size_t nkeys, void *stream) {
+    CUDIL_ENGINE_DISPATCH(e, update_secret_keys(d_sk, first, nkeys, (cudaStream_t)stream));
+}
+
 int cudil_engine_set_public_keys(cudil_engine *e, const uint8_t *d_pk, size_t nkeys, void *stream) {
     CUDIL_ENGINE_DISPATCH(e, set_public_keys(d_pk, nkeys, (cudaStream_t)stream));
 }

@@ -202,14 +202,30 @@ struct EngineImpl : EngineBase {
 
     int set_secret_keys(const uint8_t *d_sk, size_t nkeys, cudaStream_t st) {
         if (!d_sk || nkeys == 0 || nkeys > max_keys || !owns_cache) return CUDIL_ERR_INVALID;
+        const int rc = build_sk_rows(d_sk, 0, nkeys, st);
+        if (rc == CUDIL_OK) n_sk = nkeys;
+        return rc;
+    }
+
+    // Cache rows [first, first + nkeys); first <= the number of rows built so far, so the built rows
+    // stay one contiguous prefix.
+    int update_secret_keys(const uint8_t *d_sk, size_t first, size_t nkeys, cudaStream_t st) {
+        if (!d_sk || nkeys == 0 || first > n_sk || first > max_keys || nkeys > max_keys - first || !owns_cache)
+            return CUDIL_ERR_INVALID;
+        const int rc = build_sk_rows(d_sk, first, nkeys, st);
+        if (rc == CUDIL_OK) n_sk = std::max(n_sk, first + nkeys);
+        return rc;
+    }
+
+    int build_sk_rows(const uint8_t *d_sk, size_t first, size_t nkeys, cudaStream_t st) {
         const int nn = (int)nkeys;
+        uint8_t *rows = sk_cache + first * sk_pitch;
         CUDIL_LAUNCH(KID_CACHE_SK, st,
-                     k_cache_sk<MODE><<<blocks_for(nkeys * (PM::L + 2 * PM::K + 1) * 16), kBlock, 0, st>>>(d_sk, sk_cache, sk_pitch, nn));
+                     k_cache_sk<MODE><<<blocks_for(nkeys * (PM::L + 2 * PM::K + 1) * 16), kBlock, 0, st>>>(d_sk, rows, sk_pitch, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_EXPAND_A, st,
-                     k_expand_a<MODE><<<blocks_for(nkeys * PM::K * PM::L), kBlock, 0, st>>>(sk_cache, sk_pitch, C::SK_RHO, C::SK_MAT, nn));
+                     k_expand_a<MODE><<<blocks_for(nkeys * PM::K * PM::L), kBlock, 0, st>>>(rows, sk_pitch, C::SK_RHO, C::SK_MAT, nn));
         CUDIL_CK_LAUNCH();
-        n_sk = nkeys;
         return CUDIL_OK;
     }
 
@@ -326,11 +342,27 @@ struct EngineImpl : EngineBase {
             d_msgs = reinterpret_cast<const uint8_t *>(items);  // any aligned pointer; never read
         }
         if (((uintptr_t)d_msgs) & 7u) return CUDIL_ERR_INVALID;
+        const bool recapture = !g_sign || g_sign_key[0] != d_sig || g_sign_key[1] != d_msgs || g_sign_key[2] != d_rhop;
+        // The signature rows may be device memory or pinned host memory (written by the signer over
+        // PCIe as each signature is found); pageable host memory is refused before anything is queued.
+        uint8_t *out = d_sig;
+        if (recapture) {
+            cudaPointerAttributes pa{};
+            if (cudaPointerGetAttributes(&pa, d_sig) != cudaSuccess) {
+                cudaGetLastError();
+                return CUDIL_ERR_INVALID;
+            }
+            if (pa.type == cudaMemoryTypeUnregistered) return CUDIL_ERR_INVALID;
+            if (pa.type == cudaMemoryTypeHost) {
+                if (!pa.devicePointer) return CUDIL_ERR_INVALID;
+                out = static_cast<uint8_t *>(pa.devicePointer);
+            }
+        }
         int rc = upload_meta(off, mlen, key, n, n_sk, msgs_bytes, true, st);
         if (rc) return rc;
-        if (!g_sign || g_sign_key[0] != d_sig || g_sign_key[1] != d_msgs || g_sign_key[2] != d_rhop) {
+        if (recapture) {
             // for a signing graph the `sig` argument of capture carries the randomized-signing seeds
-            rc = capture(st, &g_sign, true, d_sig, d_rhop, d_msgs);
+            rc = capture(st, &g_sign, true, out, d_rhop, d_msgs);
             if (rc) return rc;
             g_sign_key[0] = d_sig;
             g_sign_key[1] = d_msgs;

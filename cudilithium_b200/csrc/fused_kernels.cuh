@@ -284,6 +284,50 @@ struct FusedSignSmem {
 
 constexpr unsigned kLockSpinLimit = 1u << 22;
 
+// Copies a staged signature (256-byte aligned words) to its output row with NT cooperating
+// threads (t = 0 .. NT-1): whole 32-bit words when the row is 4-byte aligned -- full-width writes,
+// which matters when the output is pinned host memory written over PCIe -- and bytes otherwise
+// and for a last partial word.  Eight words per thread are loaded before they are stored.
+template <int BYTES, int NT>
+__device__ __forceinline__ void publish_signature(uint8_t *dst, const uint32_t *src, int t) {
+    constexpr int NW = (BYTES + 3) / 4, NFULL = BYTES / 4;
+    if ((reinterpret_cast<uintptr_t>(dst) & 3u) == 0u) {
+        uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+#pragma unroll 1
+        for (int w0 = 0; w0 < NFULL; w0 += 8 * NT) {
+            uint32_t w[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int wi = w0 + t + NT * k;
+                w[k] = (wi < NFULL) ? src[wi] : 0u;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int wi = w0 + t + NT * k;
+                if (wi < NFULL) d[wi] = w[k];
+            }
+        }
+        if (NFULL < NW && t < BYTES - 4 * NFULL) dst[4 * NFULL + t] = (uint8_t)(src[NFULL] >> (8 * t));
+        return;
+    }
+#pragma unroll 1
+    for (int w0 = 0; w0 < NW; w0 += 8 * NT) {
+        uint32_t w[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int wi = w0 + t + NT * k;
+            w[k] = (wi < NW) ? src[wi] : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int wi = w0 + t + NT * k;
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+                if (wi < NW && 4 * wi + b < BYTES) dst[4 * wi + b] = (uint8_t)(w[k] >> (8 * b));
+        }
+    }
+}
+
 template <int MODE, int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSignArgs arg) {
     using PM = P<MODE>;
@@ -560,26 +604,8 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         if (g.t == 0) cur = *reinterpret_cast<volatile unsigned *>(arg.best + item);
         cur = __shfl_sync(g.gmask, cur, lane_off);
         if (cur == nonce) {
-            // the staged signature is 256-byte aligned; the output row may only be byte aligned
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(slot + C::SL_SIG);
-            uint8_t *dst = arg.sig_out + (size_t)item * arg.sig_pitch;
-            constexpr int NW = (PM::SIG_BYTES + 3) / 4;
-#pragma unroll 1
-            for (int w0 = 0; w0 < NW; w0 += 16 * 8) {
-                uint32_t w[8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int wi = w0 + g.t + 16 * k;
-                    w[k] = (wi < NW) ? src[wi] : 0u;
-                }
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int wi = w0 + g.t + 16 * k;
-#pragma unroll
-                    for (int b = 0; b < 4; ++b)
-                        if (wi < NW && 4 * wi + b < PM::SIG_BYTES) dst[4 * wi + b] = (uint8_t)(w[k] >> (8 * b));
-                }
-            }
+            publish_signature<PM::SIG_BYTES, 16>(arg.sig_out + (size_t)item * arg.sig_pitch,
+                                                 reinterpret_cast<const uint32_t *>(slot + C::SL_SIG), g.t);
         }
         __threadfence();
         __syncwarp(g.gmask);

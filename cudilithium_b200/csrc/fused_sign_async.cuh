@@ -502,18 +502,9 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
                 unsigned cur = 0;
                 if (lane == 0) cur = *reinterpret_cast<volatile unsigned *>(arg.best + item);
                 cur = __shfl_sync(FULL, cur, 0);
-                if (cur == nonce) {
-                    const uint32_t *src = reinterpret_cast<const uint32_t *>(slot + C::SL_SIG);
-                    uint8_t *dst = arg.sig_out + (size_t)item * arg.sig_pitch;
-                    constexpr int NWD = (PM::SIG_BYTES + 3) / 4;
-#pragma unroll 1
-                    for (int wi = lane; wi < NWD; wi += 32) {
-                        const uint32_t w = src[wi];
-#pragma unroll
-                        for (int b = 0; b < 4; ++b)
-                            if (4 * wi + b < PM::SIG_BYTES) dst[4 * wi + b] = (uint8_t)(w >> (8 * b));
-                    }
-                }
+                if (cur == nonce)
+                    publish_signature<PM::SIG_BYTES, 32>(arg.sig_out + (size_t)item * arg.sig_pitch,
+                                                         reinterpret_cast<const uint32_t *>(slot + C::SL_SIG), lane);
                 __threadfence();
                 __syncwarp();
                 if (lane == 0) atomicExch(arg.locks + item, 0u);

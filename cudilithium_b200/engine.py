@@ -91,6 +91,13 @@ class Engine:
         n = d_sk.numel() // self.params.sk_bytes
         check(lib.cudil_engine_set_secret_keys(self.h, d_sk.data_ptr(), n, _sp(stream)), "set_secret_keys")
 
+    def update_secret_keys(self, d_sk: torch.Tensor, first: int, stream=None):
+        """Cache rows first .. first + n - 1 from the n packed secret keys in d_sk (first must not
+        exceed the rows built so far); see cudil_engine_update_secret_keys."""
+        n = d_sk.numel() // self.params.sk_bytes
+        check(lib.cudil_engine_update_secret_keys(self.h, d_sk.data_ptr(), first, n, _sp(stream)),
+              "update_secret_keys")
+
     def attach_keys(self, src: "Engine"):
         """Share src's key caches (same parameter set); src must outlive this engine."""
         check(lib.cudil_engine_attach_keys(self.h, src.h), "attach_keys")

@@ -201,7 +201,10 @@ int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t
  * sign/verify: d_msgs is one device buffer of msgs_bytes bytes holding every message at an 8-byte
  *          aligned offset (offsets[i] + mlens[i] <= msgs_bytes, checked before any launch);
  *          offsets / mlens / key_idx are HOST arrays of n entries (uploaded before the launch);
- *          signatures are dense (sig_bytes each).  Asynchronous on `stream`; one batch in flight
+ *          signatures are dense (sig_bytes each).  The signature output of sign may be device
+ *          memory or pinned host memory: in host memory each signature is written over PCIe as
+ *          soon as it is found, so the download overlaps the signing (pageable host memory:
+ *          CUDIL_ERR_INVALID).  Asynchronous on `stream`; one batch in flight
  *          per engine (calls on one engine must be ordered on one stream).
  * last_status: attempts and error flags of the last completed batch (valid after sync);
  *          returns CUDIL_ERR_TIMEOUT if a bounded device wait gave up. */
@@ -211,6 +214,11 @@ int cudil_engine_create(cudil_engine **out, int mode, size_t max_keys, size_t ma
 int cudil_engine_destroy(cudil_engine *e);
 size_t cudil_engine_device_bytes(const cudil_engine *e);
 int cudil_engine_set_secret_keys(cudil_engine *e, const uint8_t *d_sk, size_t nkeys, void *stream);
+/* Builds the cache rows of keys first .. first + nkeys - 1 from nkeys packed secret keys at d_sk
+ * (first must not exceed the number of rows built so far, so the built rows stay a prefix), e.g.
+ * to replace some keys of a resident table, or to build the table in chunks, each chunk's build
+ * queued behind its own host-to-device copy so the copies of later chunks overlap it. */
+int cudil_engine_update_secret_keys(cudil_engine *e, const uint8_t *d_sk, size_t first, size_t nkeys, void *stream);
 /* Share src's key caches (same parameter set; src must outlive e).  An engine created with
  * max_keys = 0 owns no caches and must attach before signing or verifying. */
 int cudil_engine_attach_keys(cudil_engine *e, const cudil_engine *src);
