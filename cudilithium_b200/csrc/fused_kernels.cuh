@@ -348,6 +348,21 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
     Group g;
     g.t = tid & 15;
     g.gmask = 0xFFFFu << lane_off;
+    // Dilithium2's signer holds the inlined transforms in its register budget without spilling, so
+    // loads issued before a transform overlap it; the larger parameter sets call the out-of-line
+    // copies, which keep register use and code size down.
+    auto fwd = [&](int32_t (&x)[16]) {
+        if constexpr (MODE == 2)
+            ntt16s(x, g.sm, g.gmask, g.t);
+        else
+            ntt16_ool(x, g.sm, g.gmask, g.t);
+    };
+    auto inv = [&](int32_t (&x)[16]) {
+        if constexpr (MODE == 2)
+            intt16s(x, g.sm, g.gmask, g.t);
+        else
+            intt16_ool(x, g.sm, g.gmask, g.t);
+    };
 
     // ---------------- claim: fill batch `buf` with up to A attempts of this block's items
     // (block-collective; warp 0 scans the owned items, one item per lane per pass)
@@ -478,7 +493,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         }
         int32_t ch[16];
         challenge_strided(ch, masks, g.t);
-        ntt16_ool(ch, g.sm, g.gmask, g.t);
+        fwd(ch);
         const int32_t *s1 = reinterpret_cast<const int32_t *>(row + C::SK_S1);
         const int32_t *s2 = reinterpret_cast<const int32_t *>(row + C::SK_S2);
         const int32_t *t0 = reinterpret_cast<const int32_t *>(row + C::SK_T0);
@@ -488,7 +503,9 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         int32_t nx[16];
         // Acceptance needs every check to pass, so the checks run most selective first: steps
         // r0_0..r0_{K-1} (r0 replaces w0 in the slot, for the hints), z_0..z_{L-1}, then
-        // ct0_0..ct0_{K-1} with the hints; the next step's operand loads while one transforms.
+        // ct0_0..ct0_{K-1} with the hints.  While one step transforms, the next step's key
+        // operand and (inlined transforms) this step's slot data (y_j, or w0_i / r0_i) are in
+        // flight.
         auto operand = [&](int step) -> const int32_t * {
             if (step < K) return s2 + (size_t)step * N;
             if (step < K + L) return s1 + (size_t)(step - K) * N;
@@ -503,16 +520,27 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], nx[m]);
             if (step + 1 < L + 2 * K) load16_contig(nx, operand(step + 1) + 16 * g.t);
-            intt16_ool(x, g.sm, g.gmask, g.t);
+            // slot data of this step (y_j, or w0_i / r0_i); with the out-of-line transform a load in
+            // flight across the call would be spilled, so there it is read after the transform
+            const int32_t *w0c = reinterpret_cast<const int32_t *>(slot + C::SL_W0) + (size_t)i * N;
+            int32_t pre[16];
+            if constexpr (MODE == 2) {
+                if (is_z) {
+                    unpack_z_strided<MODE>(pre, slot + C::SL_Y + (size_t)(step - K) * PM::POLYZ_PACKED, g.t);
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) pre[m] = w0c[g.t + 16 * m];
+                }
+            }
+            inv(x);
             ++n_intt;
             bool bad = false;
             if (is_z) {
                 const int j = step - K;
-                int32_t y[16];
-                unpack_z_strided<MODE>(y, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
+                if constexpr (MODE != 2) unpack_z_strided<MODE>(pre, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
-                    x[m] = reduce32(x[m] + y[m]);
+                    x[m] = reduce32(x[m] + pre[m]);
                     bad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
                 }
                 if (group_any(g, bad)) {
@@ -531,7 +559,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                 int32_t r0[16];
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
-                    r0[m] = reduce32(w0[g.t + 16 * m] - x[m]);
+                    r0[m] = reduce32((MODE == 2 ? pre[m] : w0c[g.t + 16 * m]) - x[m]);
                     bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
                 }
                 if (group_any(g, bad)) {
@@ -550,12 +578,11 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                     rejected = true;
                     break;
                 }
-                const int32_t *r0p = reinterpret_cast<const int32_t *>(slot + C::SL_W0) + (size_t)i * N;
                 const uint8_t *w1p = slot + C::SL_W1P + (size_t)i * PM::POLYW1_PACKED;
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
                     const int32_t w1 = (int32_t)get_bits(w1p, (g.t + 16 * m) * PM::W1_BITS, PM::W1_BITS);
-                    const unsigned h = make_hint<MODE>(r0p[g.t + 16 * m] + x[m], w1);
+                    const unsigned h = make_hint<MODE>((MODE == 2 ? pre[m] : w0c[g.t + 16 * m]) + x[m], w1);
                     const unsigned bal = (__ballot_sync(g.gmask, h) >> lane_off) & 0xFFFFu;
                     if (h) {
                         const int idx = cnt + __popc(bal & ((1u << g.t) - 1u));
@@ -626,7 +653,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         for (int j = 0; j < L; ++j) {
             int32_t x[16];
             unpack_z_strided<MODE>(x, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
-            ntt16_ool(x, g.sm, g.gmask, g.t);
+            fwd(x);
             store16_smem(yh + j * N, x, g.t);
         }
         __syncwarp(g.gmask);
@@ -656,7 +683,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
             }
 #pragma unroll
             for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m]);
-            intt16_ool(acc, g.sm, g.gmask, g.t);
+            inv(acc);
             int32_t *w0 = reinterpret_cast<int32_t *>(slot + C::SL_W0) + (size_t)i * N;
             int32_t w1[16];
 #pragma unroll
