@@ -57,6 +57,55 @@ __device__ __forceinline__ void expand_a_stream(const uint2 (&rho)[4], int i, in
     }
 }
 
+// The same entry written to out[0..255].  Where out is 16-byte aligned, a group of eight
+// candidates that are all accepted while the count is a multiple of four goes out as two 16-byte
+// stores; anything else is stored coefficient by coefficient (a candidate is rejected with
+// probability (2^23 - q) / 2^23 < 0.1%, so nearly every group takes the wide path).
+__device__ __forceinline__ void expand_a_row(const uint2 (&rho)[4], int i, int j, int32_t *out) {
+    uint32_t al[25], ah[25];
+    shake_absorb_seed_nonce<SHAKE128_RATE, 4>(al, ah, rho, (uint32_t)((i << 8) | j));
+    const bool wide = (reinterpret_cast<uintptr_t>(out) & 15u) == 0u;
+    int ctr = 0;
+#pragma unroll 1
+    while (ctr < N) {
+        keccak_f1600(al, ah);
+#pragma unroll
+        for (int g = 0; g < 7; ++g) {
+            const uint32_t w0 = al[3 * g], w1 = ah[3 * g], w2 = al[3 * g + 1];
+            const uint32_t w3 = ah[3 * g + 1], w4 = al[3 * g + 2], w5 = ah[3 * g + 2];
+            uint32_t c[8];
+            c[0] = w0;
+            c[1] = __funnelshift_r(w0, w1, 24);
+            c[2] = __funnelshift_r(w1, w2, 16);
+            c[3] = w2 >> 8;
+            c[4] = w3;
+            c[5] = __funnelshift_r(w3, w4, 24);
+            c[6] = __funnelshift_r(w4, w5, 16);
+            c[7] = w5 >> 8;
+            bool all = true;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                c[m] &= 0x7FFFFFu;
+                all &= c[m] < (uint32_t)Q;
+            }
+            if (wide && all && (ctr & 3) == 0 && ctr + 8 <= N) {
+                int4 *o = reinterpret_cast<int4 *>(out + ctr);
+                o[0] = make_int4((int)c[0], (int)c[1], (int)c[2], (int)c[3]);
+                o[1] = make_int4((int)c[4], (int)c[5], (int)c[6], (int)c[7]);
+                ctr += 8;
+            } else {
+#pragma unroll
+                for (int m = 0; m < 8; ++m) {
+                    if (c[m] < (uint32_t)Q && ctr < N) {
+                        out[ctr] = (int32_t)c[m];
+                        ++ctr;
+                    }
+                }
+            }
+        }
+    }
+}
+
 // ExpandS entry: SHAKE256(rho' || nonce), nibbles < 15 (eta 2) or < 9 (eta 4), low nibble first
 // (src/keypair.cu:84-114).  emit(ctr, s) with s in [-eta, eta].
 template <int MODE, typename Emit>

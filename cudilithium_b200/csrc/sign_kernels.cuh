@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kBlock) k_expand_a(uint8_t *pool, size_t pitch
     uint2 rho[4];
     ld_lanes(rho, row + rho_off);
     int32_t *out = reinterpret_cast<int32_t *>(row + mat_off) + (size_t)ij * N;
-    expand_a_stream(rho, ij / L, ij % L, [&](int c, int32_t v) { out[c] = v; });
+    expand_a_row(rho, ij / L, ij % L, out);
 }
 
 // One 16-thread group per secret polynomial: unpack (eta / 13-bit) and forward NTT.
