@@ -833,7 +833,8 @@ def main():
     ap.add_argument("--engine-threads", type=int, default=0, help="fused engine block size (0 = tuned default)")
     ap.add_argument("--spec-slots", type=int, default=0, help="fused signer attempts in flight (0 = tuned default)")
     ap.add_argument("--sign-kernel", type=int, default=-1,
-                    help="fused signer kernel: 0 phased, 1 async 256/64, 2 async 512/128 (-1 = tuned default)")
+                    help="fused signer kernel: 0 phased, 1..4 async 256/64, 512/128, 640/160, 768/192, "
+                         "5 phased with one wide block per SM (-1 = tuned default)")
     ap.add_argument("--quick", action="store_true", help="headline only (skip configs 1-4)")
     ap.add_argument("--workload", default="headline",
                     choices=["headline", "serve", "fused-sign", "fused-verify", "ntt", "plain-sign"],

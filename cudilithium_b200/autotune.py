@@ -22,8 +22,9 @@ DEFAULTS = {2: {"threads": 256, "spec_slots": 32, "sign_kernel": 0},
             5: {"threads": 256, "spec_slots": 32, "sign_kernel": 0}}
 THREADS = (128, 256)
 SPEC = (16, 32, 64, 128)
-# asynchronous signer variants (kernel, speculation target = its slot count)
-ASYNC = ((2, 128), (3, 160))
+# other signer variants (kernel, speculation target): asynchronous (target = its slot count) and
+# the phased kernel with one wide block per SM
+ASYNC = ((2, 128), (3, 160), (5, 32), (5, 64), (5, 128), (5, 256))
 
 
 def _gpu_name() -> str:

@@ -41,13 +41,17 @@ struct EngineBase {
     size_t scratch_bytes = 0;
     int sign_grid = 0, verify_grid = 0, prehash_grid = 0;
     size_t sign_smem = 0, verify_smem = 0;
-    // signer kernel: 0 = phased k_fused_sign (block-wide Keccak / NTT phases); 1..4 = asynchronous
-    // k_fused_sign_async with (threads, slots) per block of (256, 64), (512, 128), (640, 160),
-    // (768, 192)
+    // signer kernel: 0 = phased k_fused_sign (block-wide Keccak / NTT phases) with the engine's
+    // block size; 1..4 = asynchronous k_fused_sign_async with (threads, slots) per block of
+    // (256, 64), (512, 128), (640, 160), (768, 192); 5 = phased with one wide block per SM (512
+    // threads, 384 for Dilithium5, whose wider phase buffers allow no more)
     int sign_kernel = 0;
     static constexpr int kAsyncVariants = 4;  // (threads, slots) = (256, 64), (512, 128), (640, 160), (768, 192)
+    static constexpr int kWideVariant = kAsyncVariants + 1;
     int async_grid[kAsyncVariants] = {0, 0, 0, 0};
     size_t async_smem[kAsyncVariants] = {0, 0, 0, 0};
+    int wide_grid = 0;
+    size_t wide_smem = 0;
     // instantiated graphs, keyed by the output / message buffers they were captured with
     cudaGraphExec_t g_sign = nullptr, g_verify = nullptr;
     const void *g_sign_key[3] = {nullptr, nullptr, nullptr}, *g_verify_key[2] = {nullptr, nullptr};
@@ -86,7 +90,19 @@ struct EngineImpl : EngineBase {
         size_t b = std::max((size_t)sign_grid * 2 * threads * C::SLOT, (size_t)verify_grid * threads * C::VSLOT);
         static constexpr int slots[kAsyncVariants] = {64, 128, 160, 192};
         for (int v = 0; v < kAsyncVariants; ++v) b = std::max(b, (size_t)async_grid[v] * slots[v] * C::SLOT);
+        b = std::max(b, (size_t)wide_grid * 2 * kWideThreads * C::SLOT);
         return b;
+    }
+
+    static constexpr int kWideThreads = (MODE == 5) ? 384 : 512;
+
+    int configure_wide() {
+        wide_smem = FusedSignSmem<MODE, kWideThreads>::BYTES;
+        if (cudaFuncSetAttribute(k_fused_sign<MODE, kWideThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)wide_smem) != cudaSuccess)
+            return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
+        wide_grid = grid_for<kWideThreads>((const void *)k_fused_sign<MODE, kWideThreads>, wide_smem, sm_count);
+        return wide_grid > 0 ? CUDIL_OK : cudil_record_cuda_error(cudaErrorInvalidConfiguration, __FILE__, __LINE__);
     }
 
     template <int T, int S>
@@ -131,6 +147,8 @@ struct EngineImpl : EngineBase {
         int rc = (threads == 128) ? configure<128>() : (threads == 256 ? configure<256>() : CUDIL_ERR_INVALID);
         if (rc) return rc;
         rc = configure_async();
+        if (rc) return rc;
+        rc = configure_wide();
         if (rc) return rc;
         prehash_grid = (int)std::min<size_t>((mi + kBlock - 1) / kBlock, (size_t)sm_count * 8);
         device_bytes = required_bytes(mk, mi);
@@ -294,6 +312,8 @@ struct EngineImpl : EngineBase {
             k_fused_sign_async<MODE, 640, 160><<<async_grid[2], 640, async_smem[2], st>>>(a);
         else if (sign_kernel == 4)
             k_fused_sign_async<MODE, 768, 192><<<async_grid[3], 768, async_smem[3], st>>>(a);
+        else if (sign_kernel == kWideVariant)
+            k_fused_sign<MODE, kWideThreads><<<wide_grid, kWideThreads, wide_smem, st>>>(a);
         else
             k_fused_sign<MODE, T><<<sign_grid, T, sign_smem, st>>>(a);
         cudaMemcpyAsync(h_status, q, sizeof(FusedQueue), cudaMemcpyDeviceToHost, st);
@@ -403,7 +423,7 @@ struct EngineImpl : EngineBase {
 
     // Target of signing attempts in flight; the graph is re-captured on the next batch.
     int set_sign_kernel(int v) {
-        if (v < 0 || v > kAsyncVariants) return CUDIL_ERR_INVALID;
+        if (v < 0 || v > kWideVariant) return CUDIL_ERR_INVALID;
         sign_kernel = v;
         g_sign_key[0] = nullptr;
         return CUDIL_OK;

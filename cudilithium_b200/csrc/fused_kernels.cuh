@@ -253,8 +253,8 @@ static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *loc
 // in-flight counter; a claim gives pending items (no accepted nonce yet) their next nonce, at most
 // D in flight per item, D = spec_slots / pending (1..64).  While a block owning many items has many
 // pending, D = 1 and each batch takes half of them, so the two batches in flight hold different
-// items and no attempt is wasted (blocks owning fewer than 64 items keep D >= 2 so both batches
-// stay fed); as pending items run out D grows up to 64, so the last items of a block are
+// items and no attempt is wasted (blocks owning fewer than A / 4 items keep D >= 2 so both
+// batches stay fed); as pending items run out D grows up to 64, so the last items of a block are
 // speculated deeply instead of taking one rejection round after another.
 // Nonces of an item are issued in increasing order and every issued attempt completes before the
 // block exits, so the winner -- the smallest accepted nonce -- is the deterministic signature.
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
             unsigned D = 0;
             if (pend) {
                 // depth 1 (alternating halves) needs enough owned items to fill both batches
-                const unsigned dmin = (n_own >= 64u) ? 1u : 2u;
+                const unsigned dmin = (n_own >= (unsigned)A / 4u) ? 1u : 2u;
                 const unsigned t = arg.spec_slots / pend;
                 D = t < dmin ? dmin : (t > 64u ? 64u : t);
             }

@@ -68,7 +68,8 @@ class Engine:
 
     def set_sign_kernel(self, variant: int):
         """0 phased persistent signer; 1..4 asynchronous with (threads, slots) per block of
-        (256, 64), (512, 128), (640, 160), (768, 192); see cudil_engine_set_sign_kernel."""
+        (256, 64), (512, 128), (640, 160), (768, 192); 5 phased with one wide block per SM (512
+        threads, 384 for Dilithium5); see cudil_engine_set_sign_kernel."""
         check(lib.cudil_engine_set_sign_kernel(self.h, variant), "set_sign_kernel")
 
     def last_jobs(self) -> dict:

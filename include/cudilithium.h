@@ -248,7 +248,8 @@ int cudil_engine_set_spec_slots(cudil_engine *e, unsigned spec_slots);
  * threads_per_block threads); 1..4 = asynchronous persistent kernel -- warps take ready jobs from a
  * per-block attempt-slot state machine without block barriers, the speculation target capped at
  * the slot count -- with (threads, slots) per block of (256, 64), (512, 128), (640, 160) and
- * (768, 192).  Results are identical for every variant. */
+ * (768, 192); 5 = the phased kernel with one wide block per SM (512 threads; 384 for Dilithium5).
+ * Results are identical for every variant. */
 int cudil_engine_set_sign_kernel(cudil_engine *e, int variant);
 /* Job profile of the last batch of the asynchronous signer, summed over warps: SM cycles spent in
  * rejection / w / challenge / ExpandMask jobs, claims and idle polls (out[0..5]) and their counts

@@ -127,11 +127,11 @@ def test_engine_argument_errors(cuda_ok, oracle):
 
 
 @pytest.mark.parametrize("mode", MODES)
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_engine_sign_kernel_variants_match_oracle(cuda_ok, oracle, mode, variant):
-    """Every signer kernel (phased, asynchronous 256/64, asynchronous 512/128) gives the oracle's
-    signatures: many items per block, fewer items than blocks, one item, repeated keys, uneven
-    message lengths, and a batch where several blocks own no item."""
+    """Every signer kernel (phased, the four asynchronous shapes, phased with one wide block per SM)
+    gives the oracle's signatures: many items per block, fewer items than blocks, one item,
+    repeated keys, uneven message lengths, and a batch where several blocks own no item."""
     import torch
     from cudilithium_b200.engine import Engine
     rng = np.random.default_rng(300 + 10 * mode + variant)
@@ -154,10 +154,10 @@ def test_engine_sign_kernel_variants_match_oracle(cuda_ok, oracle, mode, variant
     assert np.all(eng.verify_np(sig, msgs, key_idx) == 0)
 
 
-@pytest.mark.parametrize("variant", [1, 3])
+@pytest.mark.parametrize("variant", [1, 3, 5])
 @pytest.mark.parametrize("spec", [1, 8, 0])
 def test_engine_async_speculation_targets(cuda_ok, oracle, variant, spec):
-    """Speculation target 1 (no speculation), 8 and the slot count give the same signatures."""
+    """Speculation target 1 (no speculation), 8 and the largest one give the same signatures."""
     import torch
     from cudilithium_b200.engine import Engine
     mode, nk, n = 2, 3, 400
