@@ -50,8 +50,10 @@ OPS_PERM = 24 * 190
 OPS_NTT_FWD = 1024 * 6          # 1024 butterflies: 3 IMAD + 3 IADD
 OPS_NTT_INV = 1024 * 6 + 256 * 4  # + the final multiplication by f
 OPS_PW = 5                        # one Montgomery pointwise product
-# k_fused_sign<2,256>, batch 10000: 1.014292 GB read + 0.488978 GB written per launch (ncu)
-FUSED_SIGN_TRAFFIC_BYTES = 1.014292e9 + 0.488978e9
+# k_fused_sign<2,512> (engine sign-kernel variant 5), batch 10000: 1.035505 GB read + 0.517097 GB
+# written per launch (ncu)
+FUSED_SIGN_TRAFFIC_BYTES = 1.035505e9 + 0.517097e9
+FUSED_SIGN_TRAFFIC_VARIANT = 5
 
 
 def log(*a):
@@ -430,13 +432,15 @@ def run_gpu(args) -> dict | None:
     achieved = sign_ops / (g_ms / 1e3) / 1e9 if g_ms else None
     total_ms = sum(v[0] for v in stats.values())
     roofline = {
-        "bound": "int32-alu", "kernel": "k_fused_sign (persistent, graph with init + prehash)",
+        "bound": "int32-alu",
+        "kernel": f"persistent signer, engine sign-kernel variant {es.sign_kernel} "
+                  f"({es.info()['sign_blocks']} blocks; graph with init + prehash)",
         "achieved": achieved, "peak": peak_ops / 1e9, "unit": "Gop/s",
         "frac": achieved / (peak_ops / 1e9) if achieved else None,
         # DRAM bytes per launch of the same signer launch (batch 10000, one key per message) from
         # one ncu capture: dram__bytes_read.sum + dram__bytes_write.sum
-        "traffic": FUSED_SIGN_TRAFFIC_BYTES if (B == 10000 and mode == 2) else None,
-        "traffic_source": "ncu --set full capture of k_fused_sign<2,256>, bench.py --workload fused-sign --batch 10000",
+        "traffic": FUSED_SIGN_TRAFFIC_BYTES if (B == 10000 and mode == 2 and es.sign_kernel == FUSED_SIGN_TRAFFIC_VARIANT) else None,
+        "traffic_source": "ncu --set full capture of k_fused_sign<2,512>, bench.py --workload fused-sign --batch 10000",
         "ms_per_launch": g_ms, "launches": 1, "share_of_step": g_ms / total_ms if total_ms else None,
         "attempts": att1, "reject_intt": intt1, "signer_phases": es.last_phases(),
         "ops_model": "Keccak-f1600 = 4560 LOP3/SHF ops; NTT 6144, invNTT 7168, Montgomery product 5",

@@ -155,7 +155,9 @@ int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_
     if (threads) *threads = e->impl->threads;
     if (sign_blocks) {
         const EngineBase *b = e->impl;
-        *sign_blocks = b->sign_kernel == 0 ? b->sign_grid : b->async_grid[b->sign_kernel - 1];
+        *sign_blocks = b->sign_kernel == 0                        ? b->sign_grid
+                       : b->sign_kernel == EngineBase::kWideVariant ? b->wide_grid
+                                                                     : b->async_grid[b->sign_kernel - 1];
     }
     if (verify_blocks) *verify_blocks = e->impl->verify_grid;
     return CUDIL_OK;

@@ -71,6 +71,7 @@ class Engine:
         (256, 64), (512, 128), (640, 160), (768, 192); 5 phased with one wide block per SM (512
         threads, 384 for Dilithium5); see cudil_engine_set_sign_kernel."""
         check(lib.cudil_engine_set_sign_kernel(self.h, variant), "set_sign_kernel")
+        self.sign_kernel = variant
 
     def last_jobs(self) -> dict:
         """Asynchronous signer job profile of the last batch: {job: (cycles summed over warps, count)}."""

@@ -139,6 +139,7 @@ def test_engine_sign_kernel_variants_match_oracle(cuda_ok, oracle, mode, variant
     pk, sk = oracle.keypair_batch(mode, nk, rand_index=1300 + mode)
     eng = Engine(mode, max_keys=nk, max_items=700)
     eng.set_sign_kernel(variant)
+    assert eng.info()["sign_blocks"] > 0
     eng.set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
     for n in (700, 97, 1):
         lens = rng.integers(0, 400, n)
