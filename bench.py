@@ -50,10 +50,10 @@ OPS_PERM = 24 * 190
 OPS_NTT_FWD = 1024 * 6          # 1024 butterflies: 3 IMAD + 3 IADD
 OPS_NTT_INV = 1024 * 6 + 256 * 4  # + the final multiplication by f
 OPS_PW = 5                        # one Montgomery pointwise product
-# k_fused_sign<2,512> (engine sign-kernel variant 5), batch 10000: 1.035505 GB read + 0.517097 GB
-# written per launch (ncu)
-FUSED_SIGN_TRAFFIC_BYTES = 1.035505e9 + 0.517097e9
-FUSED_SIGN_TRAFFIC_VARIANT = 5
+# k_fused_sign<2,256> (engine sign-kernel variant 0, the tuned Dilithium2 signer), batch 10000:
+# 0.920897 GB read + 0.489304 GB written per launch (ncu)
+FUSED_SIGN_TRAFFIC_BYTES = 0.920897e9 + 0.489304e9
+FUSED_SIGN_TRAFFIC_VARIANT = 0
 
 
 def log(*a):
@@ -440,7 +440,7 @@ def run_gpu(args) -> dict | None:
         # DRAM bytes per launch of the same signer launch (batch 10000, one key per message) from
         # one ncu capture: dram__bytes_read.sum + dram__bytes_write.sum
         "traffic": FUSED_SIGN_TRAFFIC_BYTES if (B == 10000 and mode == 2 and es.sign_kernel == FUSED_SIGN_TRAFFIC_VARIANT) else None,
-        "traffic_source": "ncu --set full capture of k_fused_sign<2,512>, bench.py --workload fused-sign --batch 10000",
+        "traffic_source": "ncu --set full capture of k_fused_sign<2,256>, bench.py --workload fused-sign --batch 10000",
         "ms_per_launch": g_ms, "launches": 1, "share_of_step": g_ms / total_ms if total_ms else None,
         "attempts": att1, "reject_intt": intt1, "signer_phases": es.last_phases(),
         "ops_model": "Keccak-f1600 = 4560 LOP3/SHF ops; NTT 6144, invNTT 7168, Montgomery product 5",
