@@ -421,16 +421,21 @@ def run_gpu(args) -> dict | None:
     peak_ops = measure_alu_peak(lib, dev, spp)
     lib.cudil_kernel_stats_reset()
     lib.cudil_kernel_timing(1)
-    fused_sign()
+    # the cache build's kernels run concurrently on two streams: time the build as a whole
+    cb0, cb1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cb0.record(st)
+    es.set_secret_keys(d_sk, stream=spp)
+    cb1.record(st)
+    es.sign(f_sig, d_m, offs, lens, keys, stream=spp)
     torch.cuda.synchronize()
     lib.cudil_kernel_timing(0)
     stats = _lib.kernel_stats()
     att1, intt1 = es.last_work()
     g_ms = stats.get("k_fused_sign (graph)", (0.0, 1))[0]
     sign_ops = sign_attempt_ops(pm, att1, intt1) + B * 2 * OPS_PERM  # + mu, rho' prologue
-    c_ms = stats.get("k_cache_sk", (0.0, 1))[0] + stats.get("k_expand_a", (0.0, 1))[0]
+    c_ms = cb0.elapsed_time(cb1)
     achieved = sign_ops / (g_ms / 1e3) / 1e9 if g_ms else None
-    total_ms = sum(v[0] for v in stats.values())
+    total_ms = g_ms + c_ms  # the step: cache build span + signing graph
     roofline = {
         "bound": "int32-alu",
         "kernel": f"persistent signer, engine sign-kernel variant {es.sign_kernel} "
@@ -446,7 +451,8 @@ def run_gpu(args) -> dict | None:
         "ops_model": "Keccak-f1600 = 4560 LOP3/SHF ops; NTT 6144, invNTT 7168, Montgomery product 5",
         "peak_source": "measured live: k_alu_peak (3 LOP3 : 1 SHF at 64 ops/clk/SM; IMAD-heavy NTT work can "
                        "co-issue on the FMA pipe, so frac may exceed 1)",
-        "cache_build": {"ms": c_ms, "achieved_gops": cache_ops(pm, B) / (c_ms / 1e3) / 1e9 if c_ms else None},
+        "cache_build": {"ms": c_ms, "achieved_gops": cache_ops(pm, B) / (c_ms / 1e3) / 1e9 if c_ms else None,
+                        "note": "k_cache_sk and k_expand_a run concurrently on two streams; ms is the build's span"},
         "kernels": {k: {"ms": round(v[0], 4), "launches": v[1]} for k, v in sorted(stats.items(), key=lambda kv: -kv[1][0])},
     }
 

@@ -36,6 +36,9 @@ struct EngineBase {
     uint8_t *h_stage = nullptr;     // [FusedQueue | key | mlen | order | off]
     FusedQueue *h_status = nullptr; // D2H copy of the queue after a batch
     cudaEvent_t stage_ev = nullptr; // recorded after a batch's metadata upload from h_stage
+    // key-cache builds run their independent kernels on a side stream too (fork / join events)
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool stage_pending = false;
     uint8_t *scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -172,6 +175,9 @@ struct EngineImpl : EngineBase {
             return ::cudil::cudil_record_cuda_error(cudaGetLastError(), __FILE__, __LINE__);
         std::memset(h_status, 0, sizeof(FusedQueue));
         CUDIL_CK(cudaEventCreateWithFlags(&stage_ev, cudaEventDisableTiming));
+        CUDIL_CK(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+        CUDIL_CK(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
+        CUDIL_CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
         CUDIL_CK(cudaMemset(q, 0, sizeof(FusedQueue)));
         return CUDIL_OK;
     }
@@ -197,6 +203,9 @@ struct EngineImpl : EngineBase {
         if (h_stage) cudaFreeHost(h_stage);
         if (h_status) cudaFreeHost(h_status);
         if (stage_ev) cudaEventDestroy(stage_ev);
+        if (fork_ev) cudaEventDestroy(fork_ev);
+        if (join_ev) cudaEventDestroy(join_ev);
+        if (side) cudaStreamDestroy(side);
     }
 
     // ------------------------------------------------------------ key caches
@@ -235,29 +244,42 @@ struct EngineImpl : EngineBase {
         return rc;
     }
 
+    // The unpack / transform of s1, s2, t0 (side stream) and ExpandA (caller's stream, rho read from
+    // the packed keys) are independent and run concurrently; the caller's stream waits for both.
     int build_sk_rows(const uint8_t *d_sk, size_t first, size_t nkeys, cudaStream_t st) {
         const int nn = (int)nkeys;
         uint8_t *rows = sk_cache + first * sk_pitch;
-        CUDIL_LAUNCH(KID_CACHE_SK, st,
-                     k_cache_sk<MODE><<<blocks_for(nkeys * (PM::L + 2 * PM::K + 1) * 16), kBlock, 0, st>>>(d_sk, rows, sk_pitch, nn));
+        CUDIL_CK(cudaEventRecord(fork_ev, st));
+        CUDIL_CK(cudaStreamWaitEvent(side, fork_ev, 0));
+        CUDIL_LAUNCH(KID_CACHE_SK, side,
+                     k_cache_sk<MODE><<<blocks_for(nkeys * (PM::L + 2 * PM::K + 1) * 16), kBlock, 0, side>>>(d_sk, rows, sk_pitch, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_EXPAND_A, st,
-                     k_expand_a<MODE><<<blocks_for(nkeys * PM::K * PM::L), kBlock, 0, st>>>(rows, sk_pitch, C::SK_RHO, C::SK_MAT, nn));
+                     k_expand_a_keys<MODE><<<blocks_for(nkeys * PM::K * PM::L), kBlock, 0, st>>>(d_sk, PM::SK_BYTES, rows, sk_pitch,
+                                                                                             C::SK_MAT, nn));
         CUDIL_CK_LAUNCH();
+        CUDIL_CK(cudaEventRecord(join_ev, side));
+        CUDIL_CK(cudaStreamWaitEvent(st, join_ev, 0));
         return CUDIL_OK;
     }
 
     int set_public_keys(const uint8_t *d_pk, size_t nkeys, cudaStream_t st) {
         if (!d_pk || nkeys == 0 || nkeys > max_keys || !owns_cache) return CUDIL_ERR_INVALID;
         const int nn = (int)nkeys;
-        CUDIL_LAUNCH(KID_CACHE_PK, st, k_cache_pk_tr<MODE><<<blocks_for(nkeys), kBlock, 0, st>>>(d_pk, pk_cache, pk_pitch, nn));
+        // tr = H(pk) and t1_hat (side stream) run concurrently with ExpandA (rho from the packed keys)
+        CUDIL_CK(cudaEventRecord(fork_ev, st));
+        CUDIL_CK(cudaStreamWaitEvent(side, fork_ev, 0));
+        CUDIL_LAUNCH(KID_CACHE_PK, side, k_cache_pk_tr<MODE><<<blocks_for(nkeys), kBlock, 0, side>>>(d_pk, pk_cache, pk_pitch, nn));
         CUDIL_CK_LAUNCH();
-        CUDIL_LAUNCH(KID_CACHE_PK, st,
-                     k_cache_pk_t1<MODE><<<blocks_for(nkeys * PM::K * 16), kBlock, 0, st>>>(d_pk, pk_cache, pk_pitch, nn));
+        CUDIL_LAUNCH(KID_CACHE_PK, side,
+                     k_cache_pk_t1<MODE><<<blocks_for(nkeys * PM::K * 16), kBlock, 0, side>>>(d_pk, pk_cache, pk_pitch, nn));
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_EXPAND_A, st,
-                     k_expand_a<MODE><<<blocks_for(nkeys * PM::K * PM::L), kBlock, 0, st>>>(pk_cache, pk_pitch, C::PK_RHO, C::PK_MAT, nn));
+                     k_expand_a_keys<MODE><<<blocks_for(nkeys * PM::K * PM::L), kBlock, 0, st>>>(d_pk, PM::PK_BYTES, pk_cache, pk_pitch,
+                                                                                             C::PK_MAT, nn));
         CUDIL_CK_LAUNCH();
+        CUDIL_CK(cudaEventRecord(join_ev, side));
+        CUDIL_CK(cudaStreamWaitEvent(st, join_ev, 0));
         n_pk = nkeys;
         return CUDIL_OK;
     }

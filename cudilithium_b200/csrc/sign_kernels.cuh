@@ -79,6 +79,27 @@ __global__ void __launch_bounds__(kBlock) k_expand_a(uint8_t *pool, size_t pitch
     expand_a_row(rho, ij / L, ij % L, out);
 }
 
+// The same with rho read from the packed keys (key i at keys + i * key_bytes, rho = its first 32
+// bytes), so the build of a cache row's Â needs no other part of the row.
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_expand_a_keys(const uint8_t *keys, size_t key_bytes, uint8_t *rows, size_t pitch,
+                                                          size_t mat_off, int n) {
+    constexpr int K = Params<MODE>::K, L = Params<MODE>::L, KL = K * L;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n * KL) return;
+    const int it = s / KL, ij = s % KL;
+    const uint8_t *key = keys + (size_t)it * key_bytes;
+    uint2 rho[4];
+    if ((reinterpret_cast<uintptr_t>(key) & 7u) == 0u) {
+        ld_lanes(rho, key);
+    } else {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) rho[w] = load_lane_bytes(key + 8 * w, 8);
+    }
+    int32_t *out = reinterpret_cast<int32_t *>(rows + (size_t)it * pitch + mat_off) + (size_t)ij * N;
+    expand_a_row(rho, ij / L, ij % L, out);
+}
+
 // One 16-thread group per secret polynomial: unpack (eta / 13-bit) and forward NTT.
 template <int MODE>
 __global__ void __launch_bounds__(kBlock) k_sign_unpack_ntt(uint8_t *pool, size_t pitch, size_t mlen, int n) {
