@@ -332,7 +332,7 @@ template <int MODE, int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSignArgs arg) {
     using PM = P<MODE>;
     using C = Cache<MODE>;
-    constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA, A = THREADS, G = THREADS / 16;
+    constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA, A = THREADS;
     enum { CT_PEND = 0, CT_KJOB, CT_NJOB, CT_NA0, CT_NA1 };
     extern __shared__ __align__(16) uint8_t fs_smem[];
     unsigned *s_item = reinterpret_cast<unsigned *>(fs_smem);   // [2][A]
