@@ -131,6 +131,7 @@ SIGNATURES = {
     "cudil_engine_last_phases": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong), POINTER(c_uint32)]),
     "cudil_engine_set_spec_slots": (c_int, [c_void_p, c_uint32]),
     "cudil_engine_set_sign_kernel": (c_int, [c_void_p, c_int]),
+    "cudil_engine_set_large_batch": (c_int, [c_void_p, c_size_t, c_int, c_uint32]),
     "cudil_engine_last_jobs": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong)]),
     "cudil_engine_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "cudil_serve_trace": (c_int, [POINTER(cudil_serve_config), POINTER(c_void_p), POINTER(c_void_p),

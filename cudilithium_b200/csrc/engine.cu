@@ -148,6 +148,9 @@ int cudil_engine_last_jobs(const cudil_engine *e, unsigned long long out[12]) {
 }
 
 int cudil_engine_set_sign_kernel(cudil_engine *e, int variant) { CUDIL_ENGINE_DISPATCH(e, set_sign_kernel(variant)); }
+int cudil_engine_set_large_batch(cudil_engine *e, size_t min_items, int variant, unsigned spec_slots) {
+    CUDIL_ENGINE_DISPATCH(e, set_large_batch(min_items, variant, spec_slots));
+}
 
 int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_blocks, int *verify_blocks) {
     if (!e || !e->impl) return CUDIL_ERR_INVALID;

@@ -58,6 +58,13 @@ struct EngineBase {
     // instantiated graphs, keyed by the output / message buffers they were captured with
     cudaGraphExec_t g_sign = nullptr, g_verify = nullptr;
     const void *g_sign_key[3] = {nullptr, nullptr, nullptr}, *g_verify_key[2] = {nullptr, nullptr};
+    // Batches of at least large_min_items items (0 = never) sign with large_kernel / large_spec
+    // through a graph of their own; smaller ones with sign_kernel / spec_slots.
+    size_t large_min_items = 0;
+    int large_kernel = 0;
+    unsigned large_spec = 0;
+    cudaGraphExec_t g_sign_large = nullptr;
+    const void *g_sign_large_key[3] = {nullptr, nullptr, nullptr};
     cudaStream_t g_sign_stream = nullptr, g_verify_stream = nullptr;
     size_t device_bytes = 0;
     bool owns_cache = true;  // false when the key caches belong to another engine (attach_keys)
@@ -160,6 +167,10 @@ struct EngineImpl : EngineBase {
         pk_pitch = align256(C::PK_ROW);
         scratch_bytes = scratch_for(mi);
         spec_slots = (unsigned)threads;
+        // large batches (about 224 items per SM and more) default to the wide phased signer
+        large_min_items = (size_t)224 * (size_t)sm_count;
+        large_kernel = kWideVariant;
+        large_spec = std::min<unsigned>(128u, 2u * (unsigned)threads);
         if ((mk && (cudaMalloc(&sk_cache, mk * sk_pitch) != cudaSuccess || cudaMalloc(&pk_cache, mk * pk_pitch) != cudaSuccess)) ||
             (mi && (cudaMalloc(&items, mi * C::ITEM_BYTES) != cudaSuccess || cudaMalloc(&best, mi * sizeof(unsigned)) != cudaSuccess ||
                     cudaMalloc(&locks, mi * sizeof(unsigned)) != cudaSuccess ||
@@ -184,6 +195,7 @@ struct EngineImpl : EngineBase {
 
     ~EngineImpl() override {
         if (g_sign) cudaGraphExecDestroy(g_sign);
+        if (g_sign_large) cudaGraphExecDestroy(g_sign_large);
         if (g_verify) cudaGraphExecDestroy(g_verify);
         if (owns_cache) {
             cudaFree(sk_cache);
@@ -223,6 +235,7 @@ struct EngineImpl : EngineBase {
         n_pk = src->n_pk;
         max_keys = src->max_keys;
         g_sign_key[0] = nullptr;  // re-capture graphs with the new cache pointers
+        g_sign_large_key[0] = nullptr;
         g_verify_key[0] = nullptr;
         return CUDIL_OK;
     }
@@ -320,21 +333,22 @@ struct EngineImpl : EngineBase {
 
     // ------------------------------------------------------------ graphs
     template <int T>
-    void record_sign(cudaStream_t st, uint8_t *d_sig, const uint8_t *d_msgs, const uint8_t *d_rhop) {
+    void record_sign(cudaStream_t st, uint8_t *d_sig, const uint8_t *d_msgs, const uint8_t *d_rhop, int variant,
+                     unsigned spec) {
         MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order, d_rhop};
         k_fused_init<<<std::max(1, sm_count * 2), 256, 0, st>>>(q, best, locks, next_nonce, inflight);
         k_fused_prehash<MODE><<<prehash_grid, kBlock, 0, st>>>(sk_cache, sk_pitch, mr, items, q);
         FusedSignArgs a{sk_cache, sk_pitch, d_key, items, d_sig, (size_t)PM::SIG_BYTES, scratch, q, best, locks, next_nonce,
-                        inflight, spec_slots};
-        if (sign_kernel == 1)
+                        inflight, spec};
+        if (variant == 1)
             k_fused_sign_async<MODE, 256, 64><<<async_grid[0], 256, async_smem[0], st>>>(a);
-        else if (sign_kernel == 2)
+        else if (variant == 2)
             k_fused_sign_async<MODE, 512, 128><<<async_grid[1], 512, async_smem[1], st>>>(a);
-        else if (sign_kernel == 3)
+        else if (variant == 3)
             k_fused_sign_async<MODE, 640, 160><<<async_grid[2], 640, async_smem[2], st>>>(a);
-        else if (sign_kernel == 4)
+        else if (variant == 4)
             k_fused_sign_async<MODE, 768, 192><<<async_grid[3], 768, async_smem[3], st>>>(a);
-        else if (sign_kernel == kWideVariant)
+        else if (variant == kWideVariant)
             k_fused_sign<MODE, kWideThreads><<<wide_grid, kWideThreads, wide_smem, st>>>(a);
         else
             k_fused_sign<MODE, T><<<sign_grid, T, sign_smem, st>>>(a);
@@ -350,7 +364,8 @@ struct EngineImpl : EngineBase {
         cudaMemcpyAsync(h_status, q, sizeof(FusedQueue), cudaMemcpyDeviceToHost, st);
     }
 
-    int capture(cudaStream_t st, cudaGraphExec_t *exec, bool sign, uint8_t *out, const uint8_t *sig, const uint8_t *msgs) {
+    int capture(cudaStream_t st, cudaGraphExec_t *exec, bool sign, uint8_t *out, const uint8_t *sig, const uint8_t *msgs,
+                int variant = 0, unsigned spec = 0) {
         // graphs are captured on a private stream and launched on the caller's stream
         cudaStream_t cs;
         CUDIL_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
@@ -358,7 +373,8 @@ struct EngineImpl : EngineBase {
         cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             if (sign)
-                (threads == 128) ? record_sign<128>(cs, out, msgs, sig) : record_sign<256>(cs, out, msgs, sig);
+                (threads == 128) ? record_sign<128>(cs, out, msgs, sig, variant, spec)
+                                 : record_sign<256>(cs, out, msgs, sig, variant, spec);
             else
                 (threads == 128) ? record_verify<128>(cs, reinterpret_cast<int *>(out), sig, msgs)
                                  : record_verify<256>(cs, reinterpret_cast<int *>(out), sig, msgs);
@@ -384,7 +400,10 @@ struct EngineImpl : EngineBase {
             d_msgs = reinterpret_cast<const uint8_t *>(items);  // any aligned pointer; never read
         }
         if (((uintptr_t)d_msgs) & 7u) return CUDIL_ERR_INVALID;
-        const bool recapture = !g_sign || g_sign_key[0] != d_sig || g_sign_key[1] != d_msgs || g_sign_key[2] != d_rhop;
+        const bool large = large_min_items && n >= large_min_items;
+        cudaGraphExec_t &graph = large ? g_sign_large : g_sign;
+        const void **gkey = large ? g_sign_large_key : g_sign_key;
+        const bool recapture = !graph || gkey[0] != d_sig || gkey[1] != d_msgs || gkey[2] != d_rhop;
         // The signature rows may be device memory or pinned host memory (written by the signer over
         // PCIe as each signature is found); pageable host memory is refused before anything is queued.
         uint8_t *out = d_sig;
@@ -404,13 +423,14 @@ struct EngineImpl : EngineBase {
         if (rc) return rc;
         if (recapture) {
             // for a signing graph the `sig` argument of capture carries the randomized-signing seeds
-            rc = capture(st, &g_sign, true, out, d_rhop, d_msgs);
+            rc = capture(st, &graph, true, out, d_rhop, d_msgs, large ? large_kernel : sign_kernel,
+                         large ? large_spec : spec_slots);
             if (rc) return rc;
-            g_sign_key[0] = d_sig;
-            g_sign_key[1] = d_msgs;
-            g_sign_key[2] = d_rhop;
+            gkey[0] = d_sig;
+            gkey[1] = d_msgs;
+            gkey[2] = d_rhop;
         }
-        CUDIL_LAUNCH(KID_FUSED_SIGN, st, cudaGraphLaunch(g_sign, st));
+        CUDIL_LAUNCH(KID_FUSED_SIGN, st, cudaGraphLaunch(graph, st));
         CUDIL_CK_LAUNCH();
         Profiler::get().launches.fetch_add(2);  // the graph holds init + prehash + sign kernels
         return CUDIL_OK;
@@ -454,6 +474,15 @@ struct EngineImpl : EngineBase {
     int set_spec_slots(unsigned v) {
         spec_slots = v ? std::min<unsigned>(v, 2u * (unsigned)threads) : (unsigned)threads;
         g_sign_key[0] = nullptr;
+        return CUDIL_OK;
+    }
+
+    int set_large_batch(size_t min_items, int variant, unsigned spec) {
+        if (variant < 0 || variant > kWideVariant) return CUDIL_ERR_INVALID;
+        large_min_items = min_items;
+        large_kernel = variant;
+        large_spec = spec ? std::min<unsigned>(spec, 2u * (unsigned)threads) : (unsigned)threads;
+        g_sign_large_key[0] = nullptr;
         return CUDIL_OK;
     }
 };

@@ -73,6 +73,10 @@ class Engine:
         check(lib.cudil_engine_set_sign_kernel(self.h, variant), "set_sign_kernel")
         self.sign_kernel = variant
 
+    def set_large_batch(self, min_items: int, variant: int = 5, spec_slots: int = 128):
+        """Signer for batches of at least min_items items (0 = off); see cudil_engine_set_large_batch."""
+        check(lib.cudil_engine_set_large_batch(self.h, min_items, variant, spec_slots), "set_large_batch")
+
     def last_jobs(self) -> dict:
         """Asynchronous signer job profile of the last batch: {job: (cycles summed over warps, count)}."""
         v = (ctypes.c_ulonglong * 12)()

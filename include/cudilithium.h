@@ -251,6 +251,12 @@ int cudil_engine_set_spec_slots(cudil_engine *e, unsigned spec_slots);
  * (768, 192); 5 = the phased kernel with one wide block per SM (512 threads; 384 for Dilithium5).
  * Results are identical for every variant. */
 int cudil_engine_set_sign_kernel(cudil_engine *e, int variant);
+/* Large batches: a signing batch of at least min_items items runs signer kernel `variant` with
+ * speculation target `spec_slots` (0 = threads_per_block) through a graph of its own; smaller
+ * batches keep the kernel and target set above.  min_items = 0 turns the large-batch choice off.
+ * Default: min_items = 224 items per SM, variant 5 (the wide phased kernel), target 128, which is
+ * the fastest signer at 64 Ki items for every parameter set.  Results are identical either way. */
+int cudil_engine_set_large_batch(cudil_engine *e, size_t min_items, int variant, unsigned spec_slots);
 /* Job profile of the last batch of the asynchronous signer, summed over warps: SM cycles spent in
  * rejection / w / challenge / ExpandMask jobs, claims and idle polls (out[0..5]) and their counts
  * (out[6..11]; challenge and ExpandMask count attempts). */

@@ -155,6 +155,26 @@ def test_engine_sign_kernel_variants_match_oracle(cuda_ok, oracle, mode, variant
     assert np.all(eng.verify_np(sig, msgs, key_idx) == 0)
 
 
+@pytest.mark.parametrize("large", [(100, 5, 128), (100, 2, 0), (0, 5, 0)])
+def test_engine_large_batch_class(cuda_ok, oracle, large):
+    """Batches at or above the large-batch threshold sign through the large-batch kernel and graph,
+    smaller ones through the default: sizes alternate between the classes on one engine, and every
+    result equals the oracle."""
+    import torch
+    from cudilithium_b200.engine import Engine
+    mode, nk = 2, 4
+    rng = np.random.default_rng(900 + large[1])
+    pk, sk = oracle.keypair_batch(mode, nk, rand_index=3100)
+    eng = Engine(mode, max_keys=nk, max_items=300)
+    eng.set_large_batch(*large)
+    eng.set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
+    for n in (300, 40, 100, 99, 250):
+        msgs = rand_msgs(rng, n, rng.integers(0, 200, n))
+        key_idx = rng.integers(0, nk, n).astype(np.uint32)
+        assert np.array_equal(eng.sign_np(msgs, key_idx), oracle_sign(oracle, mode, sk, key_idx, msgs)), f"n={n}"
+        assert eng.last_status()[1] == 0
+
+
 @pytest.mark.parametrize("variant", [1, 3, 5])
 @pytest.mark.parametrize("spec", [1, 8, 0])
 def test_engine_async_speculation_targets(cuda_ok, oracle, variant, spec):
