@@ -388,7 +388,11 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                 for (unsigned k0 = 0; k0 < n_own && filled < cap; k0 += 32) {
                     const unsigned k = k0 + lane, i = b0 + k * grid;
                     bool ok = false;
-                    if (k < n_own && __ldcg(arg.best + i) == 0xFFFFFFFFu && __ldcg(arg.inflight + i) <= pass) ok = true;
+                    if (k < n_own) {
+                        // both loads issued together (one round trip, not two dependent ones)
+                        const unsigned bi = __ldcg(arg.best + i), fi = __ldcg(arg.inflight + i);
+                        ok = bi == 0xFFFFFFFFu && fi <= pass;
+                    }
                     const unsigned bal = __ballot_sync(0xFFFFFFFFu, ok);
                     const unsigned pos = filled + __popc(bal & ((1u << lane) - 1u));
                     if (ok && pos < cap) {

@@ -125,8 +125,15 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
                 unsigned k = start + k0 + lane;
                 if (k >= n_own) k -= n_own;
                 const unsigned i = b0 + k * grid;
-                const bool ok = (k0 + lane) < n_own && __ldcg(arg.best + i) == 0xFFFFFFFFu &&
-                                __ldcg(arg.inflight + i) <= pass;
+                // a lane with k0 + lane < n_own has k < n_own after the wrap (start < n_own), so i is an
+                // owned item; its two loads issue together (one round trip, not two dependent ones)
+                const bool valid = (k0 + lane) < n_own;
+                unsigned bi = 0u, fi = 0u;
+                if (valid) {
+                    bi = __ldcg(arg.best + i);
+                    fi = __ldcg(arg.inflight + i);
+                }
+                const bool ok = valid && bi == 0xFFFFFFFFu && fi <= pass;
                 const unsigned bal = __ballot_sync(FULL, ok);
                 const unsigned pos = filled + __popc(bal & ((1u << lane) - 1u));
                 if (ok && pos < ng) {
