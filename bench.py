@@ -151,10 +151,13 @@ def cpu_sign_rate(mode: int, budget_s: float, nthreads: int = 0) -> tuple[float,
 
 
 def headline_config(mode: int, B: int, world: int) -> dict:
-    """The headline workload, shared by both arms (the reference arm times a bounded sample of it)."""
+    """The headline workload, identical in both arms (the reference arm times a bounded sample of it;
+    what each arm runs is in its top-level "path")."""
+    sk_cache_mib = {2: 28.3, 3: 48.3, 5: 79.0}[mode] * B / 1024
     return {"workload": f"Dilithium{mode} batched sign (+ verify), batch {B} (the reference bench batch), "
                         f"{MLEN}-byte messages, one key per message",
-            "batch": B, "mlen": MLEN, "parallelism": f"replicas x{world}"}
+            "batch": B, "mlen": MLEN, "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2: the batch's secret-key caches alone are {sk_cache_mib:.0f} MiB per rank"}
 
 
 def run_reference(args) -> dict:
@@ -179,8 +182,8 @@ def run_reference(args) -> dict:
         "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (reference seed scheme)",
-        "config": dict(headline_config(mode, args.batch, 1),
-                       path="CPU implementation of the path (the oracle port; the reference ships no CPU Dilithium)"),
+        "config": headline_config(mode, args.batch, 1),
+        "path": "CPU implementation of the path (the oracle port; the reference ships no CPU Dilithium)",
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{n} of the workload's {args.batch} signatures per step (keys and messages of "
                                    f"the reference seed scheme), OpenMP over {cores} threads"},
@@ -188,20 +191,68 @@ def run_reference(args) -> dict:
     }
 
 
-# ---------------------------------------------------------------------------- GPU leg
-def sign_attempt_ops(pm, attempts: int, reject_intt: int) -> float:
-    """Algorithmic 32-bit ALU operations of the signing attempts of one batch (work the
-    deterministic signing algorithm performs on these attempts, early exits included)."""
+# ---------------------------------------------------------------------------- work models
+def perms_absorb(nbytes: int, rate: int = 136) -> int:
+    """Keccak-f[1600] permutations of one SHAKE absorb of nbytes (the padding block included)."""
+    return nbytes // rate + 1
+
+
+def sign_attempt_ops(pm, attempts: float, reject_intt: float) -> float:
+    """Algorithmic 32-bit ALU operations of `attempts` signing attempts whose rejection checks ran
+    `reject_intt` inverse NTTs (early exits included)."""
     K, L, w1 = pm.k, pm.l, pm.k * pm.polyw1_packed
-    perms = L * 5 + (64 + w1) // 136 + 1 + 1          # ExpandMask, c~ absorb, SampleInBall
+    perms = L * 5 + perms_absorb(64 + w1) + 1          # ExpandMask, c~ absorb, SampleInBall
     per_attempt = (perms * OPS_PERM + L * OPS_NTT_FWD + K * OPS_NTT_INV + K * L * 256 * OPS_PW  # w = A y
                    + OPS_NTT_FWD)                                                              # NTT(c)
     return attempts * per_attempt + reject_intt * (OPS_NTT_INV + 256 * OPS_PW)
 
 
+def sign_prehash_ops(mlen: int) -> float:
+    """mu = H(tr || m) and rho' = H(K || mu) of one message."""
+    return (perms_absorb(32 + mlen) + 1) * OPS_PERM
+
+
 def cache_ops(pm, nkeys: int) -> float:
     """ExpandA (K*L entries of 5 SHAKE128 blocks) + NTT of s1, s2, t0 per key."""
     return nkeys * (pm.k * pm.l * 5 * OPS_PERM + (pm.l + 2 * pm.k) * OPS_NTT_FWD)
+
+
+def keygen_ops(pm) -> float:
+    """One key pair: seed expansion, ExpandA, ExpandS (2 SHAKE256 blocks per polynomial),
+    t = invNTT(A NTT(s1)) + s2, tr = H(pk)."""
+    K, L = pm.k, pm.l
+    perms = 1 + K * L * 5 + (K + L) * 2 + perms_absorb(pm.pk_bytes)
+    return perms * OPS_PERM + L * OPS_NTT_FWD + K * OPS_NTT_INV + K * L * 256 * OPS_PW
+
+
+def verify_ops(pm, mlen: int, cached: bool) -> float:
+    """One verification; cached = A_hat, NTT(t1 2^d) and tr resident per key (no ExpandA, no H(pk))."""
+    K, L, w1 = pm.k, pm.l, pm.k * pm.polyw1_packed
+    perms = perms_absorb(32 + mlen) + perms_absorb(64 + w1) + 1
+    ntt = (L + 1) * OPS_NTT_FWD + K * OPS_NTT_INV + (K * L + K) * 256 * OPS_PW
+    if not cached:
+        perms += perms_absorb(pm.pk_bytes) + K * L * 5
+        ntt += K * OPS_NTT_FWD
+    return perms * OPS_PERM + ntt
+
+
+def algorithmic_attempts(nonces, issued: int, reject_intt: int) -> tuple[float, float]:
+    """Attempts deterministic signing needs (winning nonce + 1 per item) and the rejection checks'
+    inverse NTTs scaled to them from the issued (speculative) attempts' device count."""
+    alg = float((nonces.astype("float64") + 1.0).sum())
+    return alg, (reject_intt * alg / issued if issued else 0.0)
+
+
+def alu_roofline(ops: float, ms: float, peak_ops: float, what: str) -> dict:
+    a = ops / (ms / 1e3) / 1e9 if ms else None
+    return {"bound": "int32-alu", "what": what, "achieved": a, "peak": peak_ops / 1e9, "unit": "Gop/s",
+            "frac": a / (peak_ops / 1e9) if a else None, "peak_source": "measured live (k_alu_peak)"}
+
+
+def timed_cpu(fn):
+    t = time.perf_counter()
+    r = fn()
+    return r, time.perf_counter() - t
 
 
 class Timer:
@@ -431,8 +482,10 @@ def run_gpu(args) -> dict | None:
     lib.cudil_kernel_timing(0)
     stats = _lib.kernel_stats()
     att1, intt1 = es.last_work()
+    alg_att, alg_intt = algorithmic_attempts(es.last_nonces(B), att1, intt1)
     g_ms = stats.get("k_fused_sign (graph)", (0.0, 1))[0]
-    sign_ops = sign_attempt_ops(pm, att1, intt1) + B * 2 * OPS_PERM  # + mu, rho' prologue
+    # algorithmic work: the attempts deterministic signing needs (not the speculative ones issued)
+    sign_ops = sign_attempt_ops(pm, alg_att, alg_intt) + B * sign_prehash_ops(MLEN)
     c_ms = cb0.elapsed_time(cb1)
     achieved = sign_ops / (g_ms / 1e3) / 1e9 if g_ms else None
     total_ms = g_ms + c_ms  # the step: cache build span + signing graph
@@ -447,7 +500,10 @@ def run_gpu(args) -> dict | None:
         "traffic": FUSED_SIGN_TRAFFIC_BYTES if (B == 10000 and mode == 2 and es.sign_kernel == FUSED_SIGN_TRAFFIC_VARIANT) else None,
         "traffic_source": "ncu --set full capture of k_fused_sign<2,256>, bench.py --workload fused-sign --batch 10000",
         "ms_per_launch": g_ms, "launches": 1, "share_of_step": g_ms / total_ms if total_ms else None,
-        "attempts": att1, "reject_intt": intt1, "signer_phases": es.last_phases(),
+        "attempts_algorithmic": alg_att, "attempts_issued": att1, "speculation_overhead": att1 / alg_att,
+        "reject_intt_issued": intt1, "signer_phases": es.last_phases(),
+        "work_basis": "attempts = sum over items of (winning nonce + 1), read back from the engine; "
+                      "rejection inverse NTTs scaled from the issued attempts' device count",
         "ops_model": "Keccak-f1600 = 4560 LOP3/SHF ops; NTT 6144, invNTT 7168, Montgomery product 5",
         "peak_source": "measured live: k_alu_peak (3 LOP3 : 1 SHF at 64 ops/clk/SM; IMAD-heavy NTT work can "
                        "co-issue on the FMA pipe, so frac may exceed 1)",
@@ -460,17 +516,17 @@ def run_gpu(args) -> dict | None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": (fs_ms + fv_ms) / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic: keys from the reference seed scheme, uniform random 32-byte messages",
-        "config": dict(headline_config(mode, B, world),
-                       path="fused engine: per step the batch's key caches are built and the batch is signed in one "
-                            "graph launch (persistent signer)",
-                       engine=es.info(),
-                       l2=f"inputs larger than L2: the batch's secret-key caches alone are "
-                          f"{B * (pm.k * pm.l + pm.l + 2 * pm.k) * 1024 / 2**20:.0f} MiB per rank"),
+        "config": headline_config(mode, B, world),
+        "path": "fused engine: per step the batch's key caches are built and the batch is signed in one graph "
+                "launch (persistent signer)",
+        "engine": es.info(),
         "verify_per_s": verify_rate, "keygen_per_s": world * B / (keygen_ms / 1e3),
         "plain": {"sign_per_s": plain_sign_rate, "verify_per_s": plain_verify_rate, "exec_threshold": best_T,
                   "all_verified": plain_ok},
-        "fused_over_plain": {"sign": value / plain_sign_rate, "verify": verify_rate / plain_verify_rate},
-        "bit_exact_fused_vs_plain": fused_ok, "attempts_per_signature": attempts / B,
+        "fused_over_plain": {"sign": value / plain_sign_rate, "verify": verify_rate / plain_verify_rate,
+                             "sign_resident_keys": (B / (g_ms / 1e3)) / plain_sign_rate if g_ms else None},
+        "bit_exact_fused_vs_plain": fused_ok, "attempts_per_signature": alg_att / B,
+        "attempts_issued_per_signature": attempts / B,
         "e2e": {"value": e2e, "unit": UNIT, "key_chunks": nch, "h2d_bytes_per_step": B * (MLEN + pm.sk_bytes),
                 "d2h_bytes_per_step": B * pm.sig_bytes, "signatures": "written into pinned host memory by the signer"},
         "gpu_launches": int(launches), "wall_s_timed": wall, "clocks": clk, "roofline": roofline,
@@ -480,7 +536,7 @@ def run_gpu(args) -> dict | None:
     # the other configurations (and the serving sweep, which drives the host threads hard) run in
     # the single-GPU invocation only; a multi-GPU run reports the replicated headline
     if not args.quick and world == 1:
-        result["configs"] = run_configs(args, torch, np, lib, _lib, dev, spp, rank)
+        result["configs"] = run_configs(args, torch, np, lib, _lib, dev, spp, rank, peak_ops)
         result["configs"]["serve_mixed"] = run_serve(args, np)
     if world > 1:
         dist.barrier()
@@ -491,24 +547,51 @@ def run_gpu(args) -> dict | None:
     return result if rank == 0 else None
 
 
-def run_configs(args, torch, np, lib, _lib, dev, spp, rank) -> dict:
-    """The other configurations, reported beside the headline (not the bench value)."""
+def seed_scheme_messages(n: int, mlen: int = 32, start: int = 0):
+    """Messages of the reference's test-vector scheme: SHAKE128(le64(2i))[0:mlen]."""
+    import hashlib
+
+    import numpy as np
+    return np.stack([np.frombuffer(hashlib.shake_128((2 * i).to_bytes(8, "little")).digest(mlen), dtype=np.uint8)
+                     for i in range(start, start + n)])
+
+
+def run_configs(args, torch, np, lib, _lib, dev, spp, rank, peak_ops) -> dict:
+    """The other configurations, reported beside the headline (not the bench value).  Each leg times
+    the plain and the fused GPU path where both exist, reports the algorithmic work against the
+    measured peak, and in its CPU leg times the oracle (OpenMP over all host threads) on the same
+    inputs -- a bounded sample where the whole workload would take too long -- and checks the GPU
+    outputs against it byte for byte."""
     import ctypes
 
     import cudilithium_b200 as cd
     from cudilithium_b200.api import TaskLut, alloc_pool, ntt_mul
-    from cudilithium_b200.engine import Engine, pack_messages
+    from cudilithium_b200.engine import Engine
+    from oracle import pyoracle as ora
     st = torch.cuda.current_stream()
+    cores = os.cpu_count() or 1
     out = {}
 
-    # config 1: Dilithium2 keygen + sign + verify, batch 1024 (latency of each batch call)
+    def gpu_ms(fn, reps, warm=3):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        tm = Timer(torch, st)
+        for _ in range(reps):
+            with tm:
+                fn()
+        torch.cuda.synchronize()
+        return tm.total_ms() / reps
+
+    # ---- config 1: Dilithium2 keygen + sign + verify, batch 1024, the reference seed scheme
     d = cd.Dilithium(2)
     pm = d.params
     n = 1024
     pool, kpp = alloc_pool(d.keypair_row_bytes(), n)
     pk = torch.empty(n * pm.pk_bytes, dtype=torch.uint8, device=dev)
     sk = torch.empty(n * pm.sk_bytes, dtype=torch.uint8, device=dev)
-    m = torch.randint(0, 256, (n * 32,), dtype=torch.uint8, device=dev)
+    m1_host = seed_scheme_messages(n, 32)
+    m = torch.from_numpy(m1_host.reshape(-1)).to(dev)
     offs, lens, keys = np.arange(n, dtype=np.uint64) * 32, np.full(n, 32, np.uint32), np.arange(n, dtype=np.uint32)
     s_pool, sp = alloc_pool(d.sign_row_bytes(32), n)
     t_pool, tp = alloc_pool(d.sign_temp_row_bytes(), 4096)
@@ -516,13 +599,15 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank) -> dict:
     lut = TaskLut(n, 4096)
     sig = torch.empty(n * pm.sig_bytes, dtype=torch.uint8, device=dev)
     ret = torch.empty(n, dtype=torch.int32, device=dev)
+    psig = torch.empty_like(sig)
+    pret = torch.empty_like(ret)
     es, ev = Engine(2, n, n), Engine(2, n, n)
 
     def c1_plain():
         lib.cudil_keypair_dev(2, pk.data_ptr(), sk.data_ptr(), None, pool.data_ptr(), kpp, n, spp, 0)
-        lib.cudil_sign_dev(2, sig.data_ptr(), pm.sig_bytes, m.data_ptr(), 32, 32, sk.data_ptr(), s_pool.data_ptr(),
+        lib.cudil_sign_dev(2, psig.data_ptr(), pm.sig_bytes, m.data_ptr(), 32, 32, sk.data_ptr(), s_pool.data_ptr(),
                            sp, t_pool.data_ptr(), tp, ctypes.byref(lut.c), 4096, n, spp)
-        lib.cudil_verify_dev(2, ret.data_ptr(), sig.data_ptr(), pm.sig_bytes, pm.sig_bytes, m.data_ptr(), 32, 32,
+        lib.cudil_verify_dev(2, pret.data_ptr(), psig.data_ptr(), pm.sig_bytes, pm.sig_bytes, m.data_ptr(), 32, 32,
                              pk.data_ptr(), v_pool.data_ptr(), vp, n, spp)
 
     def c1_fused():
@@ -532,47 +617,55 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank) -> dict:
         ev.set_public_keys(pk, stream=spp)
         ev.verify(ret, sig, m, offs, lens, keys, stream=spp)
 
-    res = {}
-    for name, fn in (("plain", c1_plain), ("fused", c1_fused)):
-        for _ in range(3):
-            fn()
-        torch.cuda.synchronize()
-        tm = Timer(torch, st)
-        for _ in range(5):
-            with tm:
-                fn()
-        torch.cuda.synchronize()
-        res[name + "_ms"] = tm.total_ms() / 5
-        assert int((ret != 0).sum().item()) == 0
-    res["speedup"] = res["plain_ms"] / res["fused_ms"]
+    res = {"plain_ms": gpu_ms(c1_plain, 5), "fused_ms": gpu_ms(c1_fused, 5)}
+    res["fused_over_plain"] = res["plain_ms"] / res["fused_ms"]
+    alg1, _ = algorithmic_attempts(es.last_nonces(n), *es.last_work())
+    ops1 = n * (keygen_ops(pm) + sign_prehash_ops(32) + verify_ops(pm, 32, cached=False)) \
+        + sign_attempt_ops(pm, alg1, es.last_work()[1] * alg1 / max(es.last_work()[0], 1)) + cache_ops(pm, n)
+    res["roofline"] = alu_roofline(ops1, res["fused_ms"], peak_ops, "fused: keygen + cache builds + sign + verify")
+    g_pk, g_sk = pk.cpu().numpy().reshape(n, -1), sk.cpu().numpy().reshape(n, -1)
+    g_sig, g_ret = sig.cpu().numpy().reshape(n, -1), ret.cpu().numpy()
+    fused_eq_plain = bool(torch.equal(sig, psig) and torch.equal(ret, pret))
+    (o_pk, o_sk), t_kg = timed_cpu(lambda: ora.keypair_batch(2, n))
+    o_sig, t_sg = timed_cpu(lambda: ora.sign_batch(2, m1_host, o_sk))
+    o_ret, t_vf = timed_cpu(lambda: ora.verify_batch(2, o_sig, m1_host, o_pk))
+    res["bit_exact"] = bool(fused_eq_plain and np.array_equal(g_pk, o_pk) and np.array_equal(g_sk, o_sk)
+                            and np.array_equal(g_sig, o_sig) and np.array_equal(g_ret, o_ret) and not o_ret.any())
+    res["cpu_baseline"] = {"ms": 1e3 * (t_kg + t_sg + t_vf), "keygen_per_s": n / t_kg, "sign_per_s": n / t_sg,
+                           "verify_per_s": n / t_vf, "cores": cores, "kind": "port",
+                           "sample": f"the whole workload ({n} items), OpenMP over {cores} threads"}
+    res["gpu_over_cpu"] = res["cpu_baseline"]["ms"] / res["fused_ms"]
     out["d2_keygen_sign_verify_batch1024"] = res
+    log(f"[configs] 1: plain {res['plain_ms']:.3f} ms fused {res['fused_ms']:.3f} ms bit_exact {res['bit_exact']}")
     del pool, s_pool, t_pool, v_pool, es, ev
 
-    # config 2: NTT microbench, 2^20 polynomials: NTT -> Montgomery product -> invNTT
+    # ---- config 2: NTT microbench, 2^20 polynomials: NTT -> Montgomery product -> invNTT
     npoly = 1 << 20
     g = torch.Generator(device=dev).manual_seed(42)
     a = torch.randint(0, 8380417, (npoly, 256), dtype=torch.int32, device=dev, generator=g)
     b = torch.randint(0, 8380417, (npoly, 256), dtype=torch.int32, device=dev, generator=g)
     o = torch.empty_like(a)
-    for _ in range(3):
-        ntt_mul(a, b, o)
-    torch.cuda.synchronize()
-    tm = Timer(torch, st)
-    for _ in range(10):
-        with tm:
-            ntt_mul(a, b, o)
-    torch.cuda.synchronize()
-    ms = tm.total_ms() / 10
+    ms = gpu_ms(lambda: ntt_mul(a, b, o), 10)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
     gbs = npoly * 3072 / (ms / 1e3) / 1e9
-    out["ntt_microbench_2^20"] = {"ms": ms, "polys_per_s": npoly / (ms / 1e3), "hbm_gbs": gbs,
-                                  "hbm_frac": gbs / hbm, "hbm_peak_gbs": hbm,
-                                  "peak_source": "MEASURED_PEAKS.json" if peaks else "fallback 6650",
-                                  "bytes_per_poly": 3072, "l2": "inputs 2 GiB > L2"}
+    S = 1 << 15
+    a_s, b_s, o_s = a[:S].cpu().numpy(), b[:S].cpu().numpy(), o[:S].cpu().numpy()
+    o_ref, t_ntt = timed_cpu(lambda: ora.ntt_mul_batch(a_s, b_s))
+    ntt_ops = npoly * (OPS_NTT_FWD + OPS_NTT_INV + 256 * OPS_PW)
+    out["ntt_microbench_2^20"] = {
+        "ms": ms, "polys_per_s": npoly / (ms / 1e3), "hbm_gbs": gbs, "hbm_frac": gbs / hbm, "hbm_peak_gbs": hbm,
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                     "peak_source": "MEASURED_PEAKS.json" if peaks else "fallback 6650",
+                     "alu": alu_roofline(ntt_ops, ms, peak_ops, "fwd NTT + 256 products + inv NTT per poly")},
+        "bytes_per_poly": 3072, "l2": "inputs 2 GiB > L2",
+        "bit_exact": bool(np.array_equal(o_s, o_ref)),
+        "cpu_baseline": {"polys_per_s": S / t_ntt, "cores": cores, "kind": "port",
+                         "sample": f"the first {S} of the {npoly} polynomials, OpenMP over {cores} threads"}}
+    log(f"[configs] 2: {ms:.3f} ms {gbs:.0f} GB/s bit_exact {out['ntt_microbench_2^20']['bit_exact']}")
     del a, b, o
 
-    # config 3: Dilithium3 signing of 16384 messages over 1024 keys, log-uniform 32 B .. 64 KiB
+    # ---- config 3: Dilithium3 signing of 16384 messages over 1024 keys, log-uniform 32 B .. 64 KiB
     d3 = cd.Dilithium(3)
     p3 = d3.params
     nk, nm = 1024, 16384
@@ -591,30 +684,74 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank) -> dict:
     e3 = Engine(3, nk, nm)
     s3 = torch.empty(nm * p3.sig_bytes, dtype=torch.uint8, device=dev)
     e3.set_secret_keys(sk3, stream=spp)
-    for _ in range(3):
-        e3.sign(s3, d_msgs, offs3, mlens, keys3, stream=spp)
+    ms3 = gpu_ms(lambda: e3.sign(s3, d_msgs, offs3, mlens, keys3, stream=spp), 5)
+    cms = gpu_ms(lambda: e3.set_secret_keys(sk3, stream=spp), 1, warm=0)
+    e3.sign(s3, d_msgs, offs3, mlens, keys3, stream=spp)
     torch.cuda.synchronize()
-    tm, tc = Timer(torch, st), Timer(torch, st)
-    for _ in range(5):
-        with tm:
-            e3.sign(s3, d_msgs, offs3, mlens, keys3, stream=spp)
-    with tc:
-        e3.set_secret_keys(sk3, stream=spp)
-    torch.cuda.synchronize()
-    att3, _ = e3.last_work()
-    ms3, cms = tm.total_ms() / 5, tc.total_ms()
+    iss3, intt3 = e3.last_work()
+    alg3, alg_intt3 = algorithmic_attempts(e3.last_nonces(nm), iss3, intt3)
+    ops3 = sign_attempt_ops(p3, alg3, alg_intt3) + sum(sign_prehash_ops(int(x)) for x in mlens)
+    # plain path on the same messages: pitched rows of the longest message, secret key per row
+    mmax = int(mlens.max())
+    h_msgs = d_msgs.cpu().numpy()
+    rows = np.zeros((nm, mmax), np.uint8)
+    for i in range(nm):
+        rows[i, : mlens[i]] = h_msgs[int(offs3[i]): int(offs3[i]) + int(mlens[i])]
+    d_rows = torch.from_numpy(rows.reshape(-1)).to(dev)
+    d_ml = torch.from_numpy(mlens.astype(np.int32)).to(dev)
+    sk_rows = sk3.view(nk, p3.sk_bytes)[torch.from_numpy(keys3.astype(np.int64)).to(dev)].reshape(-1).contiguous()
+    sp3, spp3 = alloc_pool(d3.sign_row_bytes(mmax), nm)
+    T3 = 16384
+    tp3, tpp3 = alloc_pool(d3.sign_temp_row_bytes(), T3)
+    lut3 = TaskLut(nm, T3)
+    s3p = torch.empty_like(s3)
+
+    def plain3():
+        _lib.check(lib.cudil_sign_dev_varlen(3, s3p.data_ptr(), p3.sig_bytes, d_rows.data_ptr(), mmax,
+                                             d_ml.data_ptr(), mmax, sk_rows.data_ptr(), sp3.data_ptr(), spp3,
+                                             tp3.data_ptr(), tpp3, ctypes.byref(lut3.c), T3, nm, spp), "sign varlen")
+
+    ms3p = gpu_ms(plain3, 3, warm=1)
+    fused_eq_plain3 = bool(torch.equal(s3, s3p))
+    del sp3, tp3, d_rows, sk_rows
     ev3 = Engine(3, nk, nm)
     ev3.set_public_keys(pk3, stream=spp)
     r3 = torch.empty(nm, dtype=torch.int32, device=dev)
     ev3.verify(r3, s3, d_msgs, offs3, mlens, keys3, stream=spp)
     torch.cuda.synchronize()
+    # CPU leg: a uniform sample (timed) plus the 16 longest messages, checked byte for byte
+    samp = np.sort(rng.choice(nm, 384, replace=False))
+    longest = np.argsort(mlens)[-16:]
+    h_sk3 = sk3.cpu().numpy().reshape(nk, -1)
+    g_s3 = s3.cpu().numpy().reshape(nm, -1)
+
+    def ora_sign3(idx):
+        mm = np.zeros((idx.size, int(mlens[idx].max())), np.uint8)
+        for r, i in enumerate(idx):
+            mm[r, : mlens[i]] = h_msgs[int(offs3[i]): int(offs3[i]) + int(mlens[i])]
+        return ora.sign_batch(3, mm, h_sk3[keys3[idx]], mlens=mlens[idx])
+
+    o_samp, t3 = timed_cpu(lambda: ora_sign3(samp))
+    o_long = ora_sign3(longest)
     out["d3_sign_16384_loguniform"] = {
         "sign_per_s_resident_keys": nm / (ms3 / 1e3), "ms_per_batch": ms3, "cache_build_ms_1024_keys": cms,
-        "sign_per_s_incl_cache_build": nm / ((ms3 + cms) / 1e3), "attempts_per_signature": att3 / nm,
-        "mean_mlen": float(mlens.mean()), "all_verified": int((r3 != 0).sum().item()) == 0}
+        "sign_per_s_incl_cache_build": nm / ((ms3 + cms) / 1e3),
+        "plain": {"ms_per_batch": ms3p, "sign_per_s": nm / (ms3p / 1e3), "exec_threshold": T3,
+                  "path": "cudil_sign_dev_varlen: per-item ExpandA and key unpack, host-driven rounds"},
+        "fused_over_plain": {"resident_keys": ms3p / ms3, "incl_cache_build": ms3p / (ms3 + cms)},
+        "attempts_per_signature": alg3 / nm, "attempts_issued_per_signature": iss3 / nm,
+        "mean_mlen": float(mlens.mean()), "max_mlen": mmax,
+        "roofline": alu_roofline(ops3, ms3, peak_ops, "fused signer, resident keys (prehash + attempts)"),
+        "bit_exact": bool(fused_eq_plain3 and np.array_equal(g_s3[samp], o_samp)
+                          and np.array_equal(g_s3[longest], o_long)),
+        "all_verified": int((r3 != 0).sum().item()) == 0,
+        "cpu_baseline": {"sign_per_s": samp.size / t3, "cores": cores, "kind": "port",
+                         "sample": f"{samp.size} messages drawn uniformly from the {nm} (same length distribution), "
+                                   f"OpenMP over {cores} threads; the 16 longest are also checked"}}
+    log(f"[configs] 3: fused {ms3:.2f} ms plain {ms3p:.2f} ms bit_exact {out['d3_sign_16384_loguniform']['bit_exact']}")
     del e3, ev3, d_msgs
 
-    # config 4: Dilithium5 verification of 65536 signatures (256 keys x 256 64-byte messages, 10% flipped)
+    # ---- config 4: Dilithium5 verification of 65536 signatures (256 keys x 256 64-byte messages, 10% flipped)
     d5 = cd.Dilithium(5)
     p5 = d5.params
     nk, nm = 256, 65536
@@ -636,24 +773,15 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank) -> dict:
     pos = rng.integers(0, p5.sig_bytes, flip.size)
     bit = rng.integers(0, 8, flip.size)
     sv = s5.view(nm, p5.sig_bytes)
-    idx_r = torch.from_numpy(flip).to(dev)
-    idx_c = torch.from_numpy(pos).to(dev)
-    sv[idx_r, idx_c] ^= torch.from_numpy((1 << bit).astype(np.uint8)).to(dev)
+    sv[torch.from_numpy(flip).to(dev), torch.from_numpy(pos).to(dev)] ^= torch.from_numpy(
+        (1 << bit).astype(np.uint8)).to(dev)
     expect_bad = np.zeros(nm, bool)
     expect_bad[flip] = True
     ev5 = Engine(5, nk, nm)
     ev5.set_public_keys(pk5, stream=spp)
     r5 = torch.empty(nm, dtype=torch.int32, device=dev)
-    for _ in range(3):
-        ev5.verify(r5, s5, m5, offs5, lens5, keys5, stream=spp)
-    torch.cuda.synchronize()
-    tm = Timer(torch, st)
-    for _ in range(5):
-        with tm:
-            ev5.verify(r5, s5, m5, offs5, lens5, keys5, stream=spp)
-    torch.cuda.synchronize()
-    fused_ms = tm.total_ms() / 5
-    got_bad = (r5.cpu().numpy() != 0)
+    fused_ms = gpu_ms(lambda: ev5.verify(r5, s5, m5, offs5, lens5, keys5, stream=spp), 5)
+    got = r5.cpu().numpy()
     # plain path on the same signatures (per-signature ExpandA and H(pk)); keys expanded per row
     pk_rows = pk5.view(nk, p5.pk_bytes)[torch.from_numpy(keys5.astype(np.int64)).to(dev)].reshape(-1).contiguous()
     v_pool, vp = alloc_pool(d5.verify_row_bytes(64), nm)
@@ -663,18 +791,24 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank) -> dict:
         lib.cudil_verify_dev(5, r5p.data_ptr(), s5.data_ptr(), p5.sig_bytes, p5.sig_bytes, m5.data_ptr(), 64, 64,
                              pk_rows.data_ptr(), v_pool.data_ptr(), vp, nm, spp)
 
-    plain5()
-    torch.cuda.synchronize()
-    tm = Timer(torch, st)
-    for _ in range(3):
-        with tm:
-            plain5()
-    torch.cuda.synchronize()
-    plain_ms = tm.total_ms() / 3
+    plain_ms = gpu_ms(plain5, 3, warm=1)
+    samp = np.sort(rng.choice(nm, 4096, replace=False))
+    h_s5 = s5.cpu().numpy().reshape(nm, -1)[samp]
+    h_m5 = m5.cpu().numpy().reshape(nm, -1)[samp]
+    h_pk5 = pk5.cpu().numpy().reshape(nk, -1)[keys5[samp]]
+    o_r5, t5 = timed_cpu(lambda: ora.verify_batch(5, h_s5, h_m5, h_pk5))
     out["d5_verify_65536_cached_keys"] = {
         "verify_per_s_fused": nm / (fused_ms / 1e3), "verify_per_s_plain": nm / (plain_ms / 1e3),
-        "speedup": plain_ms / fused_ms, "rejections_exact": bool(np.array_equal(got_bad, expect_bad)),
-        "fused_equals_plain": bool(torch.equal(r5, r5p)), "flipped": int(flip.size)}
+        "fused_over_plain": plain_ms / fused_ms, "rejections_exact": bool(np.array_equal(got != 0, expect_bad)),
+        "fused_equals_plain": bool(torch.equal(r5, r5p)), "flipped": int(flip.size),
+        "roofline": alu_roofline(nm * verify_ops(p5, 64, cached=True), fused_ms, peak_ops,
+                                 "fused verifier, cached A_hat / t1_hat / tr"),
+        "bit_exact": bool(np.array_equal(got[samp], o_r5) and torch.equal(r5, r5p)),
+        "cpu_baseline": {"verify_per_s": samp.size / t5, "cores": cores, "kind": "port",
+                         "sample": f"{samp.size} of the {nm} signatures (flipped ones included), OpenMP over "
+                                   f"{cores} threads"}}
+    log(f"[configs] 4: fused {fused_ms:.2f} ms plain {plain_ms:.2f} ms bit_exact "
+        f"{out['d5_verify_65536_cached_keys']['bit_exact']}")
     del v_pool, ev5
     torch.cuda.empty_cache()
     return out

@@ -131,6 +131,8 @@ SIGNATURES = {
     "cudil_engine_last_phases": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong), POINTER(c_uint32)]),
     "cudil_engine_set_spec_slots": (c_int, [c_void_p, c_uint32]),
     "cudil_engine_set_sign_kernel": (c_int, [c_void_p, c_int]),
+    "cudil_engine_set_limits": (c_int, [c_void_p, c_uint32, c_uint32, c_uint32]),
+    "cudil_engine_last_nonces": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
     "cudil_engine_set_large_batch": (c_int, [c_void_p, c_size_t, c_int, c_uint32]),
     "cudil_engine_last_jobs": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong)]),
     "cudil_engine_info": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),

@@ -14,6 +14,10 @@ extern template struct EngineImpl<5>;
 
 using namespace cudil;
 
+static_assert(kNonceExhausted == CUDIL_NONCE_EXHAUSTED && kNonceLimit == CUDIL_ENGINE_NONCE_LIMIT &&
+                  kLockSpinLimit == CUDIL_ENGINE_LOCK_SPINS && kAsyncIdleLimit == CUDIL_ENGINE_IDLE_POLLS,
+              "engine bounds in the C header");
+
 struct cudil_engine {
     EngineBase *impl;
 };
@@ -148,6 +152,15 @@ int cudil_engine_last_jobs(const cudil_engine *e, unsigned long long out[12]) {
 }
 
 int cudil_engine_set_sign_kernel(cudil_engine *e, int variant) { CUDIL_ENGINE_DISPATCH(e, set_sign_kernel(variant)); }
+
+int cudil_engine_set_limits(cudil_engine *e, unsigned nonce_limit, unsigned lock_spins, unsigned idle_polls) {
+    CUDIL_ENGINE_DISPATCH(e, set_limits(nonce_limit, lock_spins, idle_polls));
+}
+
+int cudil_engine_last_nonces(cudil_engine *e, unsigned *out, size_t n, void *stream) {
+    CUDIL_ENGINE_DISPATCH(e, last_nonces(out, n, (cudaStream_t)stream));
+}
+
 int cudil_engine_set_large_batch(cudil_engine *e, size_t min_items, int variant, unsigned spec_slots) {
     CUDIL_ENGINE_DISPATCH(e, set_large_batch(min_items, variant, spec_slots));
 }

@@ -29,6 +29,9 @@ struct EngineBase {
     uint8_t *items = nullptr;       // max_items * 128
     unsigned *best = nullptr, *locks = nullptr, *next_nonce = nullptr, *inflight = nullptr;
     unsigned spec_slots = 0;  // signer's target of attempts in flight (0 = default for the grid)
+    // bounds of the signer's device-side loops (FusedSignArgs)
+    unsigned nonce_limit = kNonceLimit, lock_spins = kLockSpinLimit, idle_polls = kAsyncIdleLimit;
+    size_t last_n = 0;  // items of the last signing batch
     FusedQueue *q = nullptr;
     // metadata (device) and its pinned staging
     unsigned *d_key = nullptr, *d_mlen = nullptr, *d_order = nullptr;
@@ -339,7 +342,7 @@ struct EngineImpl : EngineBase {
         k_fused_init<<<std::max(1, sm_count * 2), 256, 0, st>>>(q, best, locks, next_nonce, inflight);
         k_fused_prehash<MODE><<<prehash_grid, kBlock, 0, st>>>(sk_cache, sk_pitch, mr, items, q);
         FusedSignArgs a{sk_cache, sk_pitch, d_key, items, d_sig, (size_t)PM::SIG_BYTES, scratch, q, best, locks, next_nonce,
-                        inflight, spec};
+                        inflight, spec, nonce_limit, lock_spins, idle_polls};
         if (variant == 1)
             k_fused_sign_async<MODE, 256, 64><<<async_grid[0], 256, async_smem[0], st>>>(a);
         else if (variant == 2)
@@ -433,6 +436,28 @@ struct EngineImpl : EngineBase {
         CUDIL_LAUNCH(KID_FUSED_SIGN, st, cudaGraphLaunch(graph, st));
         CUDIL_CK_LAUNCH();
         Profiler::get().launches.fetch_add(2);  // the graph holds init + prehash + sign kernels
+        last_n = n;
+        return CUDIL_OK;
+    }
+
+    // Winning nonce per item of the last signing batch (kNonceExhausted: no accepted nonce below the
+    // limit), copied into out (host or device memory) on st; returns after the copy completed.
+    int last_nonces(unsigned *out, size_t n, cudaStream_t st) {
+        if (!out || n > last_n || !best) return CUDIL_ERR_INVALID;
+        if (n == 0) return CUDIL_OK;
+        CUDIL_CK(cudaMemcpyAsync(out, best, n * sizeof(unsigned), cudaMemcpyDefault, st));
+        CUDIL_CK(cudaStreamSynchronize(st));
+        return CUDIL_OK;
+    }
+
+    // Bounds of the signer's loops; the signing graphs are re-captured on the next batch.
+    int set_limits(unsigned nonces, unsigned spins, unsigned polls) {
+        if (nonces == 0 || nonces > kNonceLimit) return CUDIL_ERR_INVALID;
+        nonce_limit = nonces;
+        lock_spins = spins;
+        idle_polls = polls;
+        g_sign_key[0] = nullptr;
+        g_sign_large_key[0] = nullptr;
         return CUDIL_OK;
     }
 

@@ -63,7 +63,10 @@ struct Cache {
 struct FusedQueue {
     unsigned long long next_ticket;
     unsigned int done_items;
-    unsigned int error;        // bit 0: a bounded lock wait gave up
+    // bit 0: a bounded publication-lock wait gave up; bit 1: an item reached its nonce limit (with no
+    // accepted nonce its signature row is not written); bit 2: an asynchronous signer block gave up
+    // after its idle-poll limit
+    unsigned int error;
     unsigned long long attempts;
     unsigned int n;            // items in the current batch
     unsigned int pad;
@@ -270,7 +273,15 @@ struct FusedSignArgs {
     FusedQueue *q;
     unsigned *best, *locks, *next_nonce, *inflight;
     unsigned spec_slots;  // per-block target of attempts in flight (<= 2 * THREADS)
+    // bounds of the device-side loops (run-time so that a host can shorten them):
+    unsigned nonce_limit;  // nonces an item may use (the 16-bit nonce field allows 65536)
+    unsigned lock_spins;   // tries for a per-item publication lock before giving up (error bit 0)
+    unsigned idle_polls;   // empty polls before an asynchronous signer block gives up (error bit 2)
 };
+
+// Sentinel best nonce of an item that used all its nonces without an accepted attempt: below the
+// "pending" value 0xFFFFFFFF, above every real nonce, so the item counts as finished (error bit 1).
+constexpr unsigned kNonceExhausted = 0xFFFFFFFEu;
 
 template <int MODE, int THREADS>
 struct FusedSignSmem {
@@ -282,7 +293,9 @@ struct FusedSignSmem {
     static constexpr size_t BYTES = CTRL + (PH_N > PH_K ? PH_N : PH_K);
 };
 
-constexpr unsigned kLockSpinLimit = 1u << 22;
+// default bounds of the signer's loops (FusedSignArgs)
+constexpr unsigned kNonceLimit = 1u << 16;
+constexpr unsigned kLockSpinLimit = 1u << 22;  // x ~64 ns sleeps
 
 // Copies a staged signature (256-byte aligned words) to its output row with NT cooperating
 // threads (t = 0 .. NT-1): whole 32-bit words when the row is 4-byte aligned -- full-width writes,
@@ -397,16 +410,19 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                     const unsigned pos = filled + __popc(bal & ((1u << lane) - 1u));
                     if (ok && pos < cap) {
                         const unsigned nn = atomicAdd(arg.next_nonce + i, 1u);
-                        if (nn < 65536u) {
-                            atomicAdd(arg.inflight + i, 1u);
-                            s_item[buf * A + pos] = i;
+                        atomicAdd(arg.inflight + i, 1u);
+                        s_item[buf * A + pos] = i;
+                        if (nn < arg.nonce_limit) {
                             s_nonce[buf * A + pos] = nn;
                         } else {
-                            // 2^16 attempts without acceptance: never happens in practice; mark the
-                            // slot as a no-op by reusing the item with an out-of-range nonce
-                            s_item[buf * A + pos] = i;
+                            // every nonce used without acceptance (never for honest keys at the
+                            // default limit): the slot becomes a no-op, and the first lane to get
+                            // here marks the item finished so that the block can exit
                             s_nonce[buf * A + pos] = 0xFFFFFFFFu;
-                            atomicAdd(arg.inflight + i, 1u);
+                            if (atomicCAS(arg.best + i, 0xFFFFFFFFu, kNonceExhausted) == 0xFFFFFFFFu) {
+                                atomicOr(&q->error, 2u);
+                                atomicSub(&s_ctl[CT_PEND], 1u);
+                            }
                         }
                     }
                     filled += __popc(bal);
@@ -617,9 +633,11 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
             atomicAdd(&q->done_items, 1u);
             atomicSub(&s_ctl[CT_PEND], 1u);
         }
+        // (old == kNonceExhausted: the item was already counted as finished; a late acceptance
+        // below the limit still publishes its signature)
         int got = 0;
         if (g.t == 0) {
-            for (unsigned spin = 0; spin < kLockSpinLimit; ++spin) {
+            for (unsigned spin = 0; spin < arg.lock_spins; ++spin) {
                 if (atomicCAS(arg.locks + item, 0u, 1u) == 0u) {
                     got = 1;
                     break;

@@ -44,7 +44,7 @@ struct AsyncSignSmem {
     static constexpr size_t BYTES = CTRL + (size_t)NW * WA;
 };
 
-constexpr unsigned kAsyncIdleLimit = 1u << 21;  // idle polls (x ~0.3 us) before a block gives up
+constexpr unsigned kAsyncIdleLimit = 1u << 21;  // default idle polls (x ~0.3 us) before a block gives up
 
 template <int MODE, int THREADS, int NS>
 __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS) k_fused_sign_async(FusedSignArgs arg) {
@@ -139,13 +139,18 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
                 if (ok && pos < ng) {
                     const unsigned sl = grab[pos];
                     const unsigned nn = atomicAdd(arg.next_nonce + i, 1u);
-                    if (nn < 65536u) {
+                    if (nn < arg.nonce_limit) {
                         atomicAdd(arg.inflight + i, 1u);
                         s_item[sl] = i;
                         s_nonce[sl] = nn;
                     } else {
-                        s_item[sl] = 0xFFFFFFFFu;  // 2^16 rejected attempts: the item cannot finish
-                        atomicOr(&q->error, 2u);
+                        // every nonce used without acceptance: no attempt; the first lane to get here
+                        // marks the item finished (error bit 1) so that the block can exit
+                        s_item[sl] = 0xFFFFFFFFu;
+                        if (atomicCAS(arg.best + i, 0xFFFFFFFFu, kNonceExhausted) == 0xFFFFFFFFu) {
+                            atomicOr(&q->error, 2u);
+                            atomicSub(&s_ctl[CT_PEND], 1u);
+                        }
                     }
                 }
                 filled = min(ng, filled + __popc(bal));
@@ -494,7 +499,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
             }
             int got = 0;
             if (lane == 0) {
-                for (unsigned spin = 0; spin < kLockSpinLimit; ++spin) {
+                for (unsigned spin = 0; spin < arg.lock_spins; ++spin) {
                     if (atomicCAS(arg.locks + item, 0u, 1u) == 0u) {
                         got = 1;
                         break;
@@ -621,7 +626,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
             }
         }
         if (ntaken == 0) {
-            if (++idle > kAsyncIdleLimit) {
+            if (++idle > arg.idle_polls) {
                 if (lane == 0) {
                     atomicOr(&q->error, 4u);
                     atomicExch(&s_ctl[CT_ERR], 1u);

@@ -192,13 +192,15 @@ struct Slot {
             const int rc = run_batch();
             if (rc) error = rc;
             const size_t n = batch.size();
+            completed->fetch_add(n);
             {
+                // busy is cleared under the same lock that published the work, after the batch is
+                // consumed, so the dispatcher never sees a free slot that still holds a batch
                 std::lock_guard<std::mutex> lk(mu);
                 has_work = false;
                 batch.clear();
+                busy = false;
             }
-            completed->fetch_add(n);
-            busy = false;
         }
     }
 
@@ -477,12 +479,14 @@ extern "C" int cudil_serve_trace(const cudil_serve_config *cfg, const uint8_t *c
                 }
                 const size_t take = std::min<size_t>(q.size(), (size_t)cfg->max_batch);
                 {
+                    // the slot is marked busy in the same locked region that publishes its work, so
+                    // a worker that wakes at once (or spuriously) cannot finish and clear busy first
                     std::lock_guard<std::mutex> lk(s->mu);
                     s->batch.assign(q.begin(), q.begin() + (long)take);
+                    s->busy = true;
                     s->has_work = true;
                 }
                 q.erase(q.begin(), q.begin() + (long)take);
-                s->busy = true;
                 s->cv.notify_one();
                 ++launched_batches;
                 progressed = true;

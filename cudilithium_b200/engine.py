@@ -144,6 +144,18 @@ class Engine:
         check(rc, "engine batch")
         return a.value, e.value
 
+    def set_limits(self, nonce_limit: int = 65536, lock_spins: int = 1 << 22, idle_polls: int = 1 << 21):
+        """Bounds of the signer's device-side loops (defaults restore the library's); see
+        cudil_engine_set_limits."""
+        check(lib.cudil_engine_set_limits(self.h, nonce_limit, lock_spins, idle_polls), "set_limits")
+
+    def last_nonces(self, n: int, stream=None) -> np.ndarray:
+        """Winning nonce of each of the first n items of the last signing batch (0xFFFFFFFE: the
+        item's nonces ran out); deterministic signing ran nonce + 1 attempts for the item."""
+        out = np.zeros(max(n, 1), np.uint32)
+        check(lib.cudil_engine_last_nonces(self.h, out.ctypes.data, n, _sp(stream)), "last_nonces")
+        return out[:n]
+
     def last_work(self) -> tuple[int, int]:
         """(attempts, inverse NTTs of the rejection checks) of the last signing batch."""
         a, i = ctypes.c_ulonglong(), ctypes.c_ulonglong()

@@ -207,7 +207,12 @@ int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t
  *          CUDIL_ERR_INVALID).  Asynchronous on `stream`; one batch in flight
  *          per engine (calls on one engine must be ordered on one stream).
  * last_status: attempts and error flags of the last completed batch (valid after sync);
- *          returns CUDIL_ERR_TIMEOUT if a bounded device wait gave up. */
+ *          returns CUDIL_ERR_TIMEOUT if a device-side loop hit its bound (cudil_engine_set_limits).
+ *          Error bits: 1 = a per-item publication-lock wait gave up (that attempt's signature is
+ *          not written); 2 = an item reached its nonce limit (if none of its nonces was accepted,
+ *          its row is not written and cudil_engine_last_nonces reports CUDIL_NONCE_EXHAUSTED); 4 = an
+ *          asynchronous signer block gave up after its idle-poll limit (its pending items stay
+ *          unsigned).  The engine stays usable after any of them. */
 typedef struct cudil_engine cudil_engine;
 int cudil_engine_create(cudil_engine **out, int mode, size_t max_keys, size_t max_items, int threads_per_block,
                         size_t device_budget_bytes);
@@ -235,6 +240,22 @@ int cudil_engine_verify(cudil_engine *e, int *d_ret, const uint8_t *d_sig, const
                         const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
                         void *stream);
 int cudil_engine_last_status(const cudil_engine *e, unsigned long long *attempts, unsigned *error);
+/* Bounds of the signer's device-side loops, from the next signing batch on (the defaults below):
+ *   nonce_limit  nonces an item may try (1 .. 65536; the reference's 16-bit nonce field allows
+ *                65536, src/api.cu:224 packs it into the low 16 bits of an exec slot);
+ *   lock_spins   tries for an item's publication lock before the attempt gives up (0 = at once);
+ *   idle_polls   empty polls before an asynchronous signer block gives up (0 = at the first).
+ * Running into a bound sets an error bit of cudil_engine_last_status instead of waiting longer. */
+#define CUDIL_ENGINE_NONCE_LIMIT 65536u
+#define CUDIL_ENGINE_LOCK_SPINS (1u << 22)
+#define CUDIL_ENGINE_IDLE_POLLS (1u << 21)
+int cudil_engine_set_limits(cudil_engine *e, unsigned nonce_limit, unsigned lock_spins, unsigned idle_polls);
+/* Winning (smallest accepted) nonce of each of the first n items of the last signing batch, copied
+ * into out (host or device memory) on `stream`; returns once the copy has completed.  Deterministic
+ * signing ran nonce + 1 attempts for the item; CUDIL_NONCE_EXHAUSTED marks an item whose nonces ran
+ * out (error bit 2). */
+#define CUDIL_NONCE_EXHAUSTED 0xFFFFFFFEu
+int cudil_engine_last_nonces(cudil_engine *e, unsigned *out, size_t n, void *stream);
 /* Work counters of the last completed signing batch: attempts run and inverse NTTs executed by the
  * rejection checks (for throughput accounting). */
 int cudil_engine_last_work(const cudil_engine *e, unsigned long long *attempts, unsigned long long *reject_intt);

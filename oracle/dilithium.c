@@ -563,29 +563,59 @@ int ora_sign(int mode, uint8_t *sig, const uint8_t *m, size_t mlen, const uint8_
 
 /* ---------------------------------------------------------------- well-formedness checks */
 
-/* Signature parse step: bit 0 = hint encoding invalid (per-poly end counts non-decreasing and at
- * most omega, positions strictly increasing inside a poly, unused slots zero: src/verify.cu:51-93),
- * bit 1 = a z coefficient with |z| >= gamma1 - beta (the z check of src/verify.cu:98-121). */
+/* Hint decode with the encoding checks of src/verify.cu:51-93: per-polynomial end counts
+ * non-decreasing and at most omega, positions strictly increasing inside a polynomial, unused
+ * slots zero.  hint (may be NULL) receives the decoded 0/1 vectors.  Returns 0 or -1.
+ *
+ * xor_lanes = 0 applies the checks as the scheme states them (every violation rejects).
+ * xor_lanes = 1 restates the reference kernel's own evaluation of them: one warp walks the
+ * positions of a polynomial (and then the padding) with lane = (j - start) mod 32, and the lanes'
+ * failure ballots are combined with XOR across the passes (src/verify.cu:66 and :85), so two
+ * violations 32 positions apart in the same polynomial, or two nonzero padding bytes 32 apart,
+ * cancel and the encoding is accepted.  The CUDA library implements the xor_lanes = 0 form; this
+ * one exists only so that tests can show where the two differ. */
+static int hint_decode(const ora_params *p, const uint8_t *hs, uint8_t (*hint)[N], int xor_lanes) {
+    int i, j, kk = 0;
+    uint32_t lanes;
+    if (hint) memset(hint, 0, (size_t)p->k * N);
+    for (i = 0; i < p->k; i++) {
+        const int end = hs[p->omega + i];
+        if (end < kk || end > p->omega) return -1;
+        lanes = 0;
+        for (j = kk + 1; j < end; j++)
+            if (hs[j] <= hs[j - 1]) {
+                if (!xor_lanes) return -1;
+                lanes ^= 1u << ((j - kk) & 31);
+            }
+        if (lanes) return -1;
+        if (hint)
+            for (j = kk; j < end; j++) hint[i][hs[j]] = 1;
+        kk = end;
+    }
+    lanes = 0;
+    for (j = kk; j < p->omega; j++)
+        if (hs[j]) {
+            if (!xor_lanes) return -1;
+            lanes ^= 1u << ((j - kk) & 31);
+        }
+    return lanes ? -1 : 0;
+}
+
+/* Hint-encoding check alone: 0 accepted, 1 rejected; xor_lanes as for hint_decode. */
+int ora_hint_check(int mode, const uint8_t *sig, int xor_lanes) {
+    ora_params p;
+    if (ora_params_get(mode, &p)) return -1;
+    return hint_decode(&p, sig + 32 + p.l * p.polyz_packed, NULL, xor_lanes) ? 1 : 0;
+}
+
+/* Signature parse step: bit 0 = hint encoding invalid (hint_decode, scheme form), bit 1 = a z
+ * coefficient with |z| >= gamma1 - beta (the z check of src/verify.cu:98-121). */
 int ora_sig_check(int mode, const uint8_t *sig) {
     ora_params p;
     int32_t z[N];
-    const uint8_t *hs;
-    int i, j, kk, st = 0;
+    int j, st = 0;
     if (ora_params_get(mode, &p)) return -1;
-    hs = sig + 32 + p.l * p.polyz_packed;
-    kk = 0;
-    for (i = 0; i < p.k && !(st & 1); i++) {
-        if (hs[p.omega + i] < kk || hs[p.omega + i] > p.omega) {
-            st |= 1;
-            break;
-        }
-        for (j = kk; j < hs[p.omega + i]; j++)
-            if (j > kk && hs[j] <= hs[j - 1]) st |= 1;
-        kk = hs[p.omega + i];
-    }
-    if (!(st & 1))
-        for (j = kk; j < p.omega; j++)
-            if (hs[j]) st |= 1;
+    if (hint_decode(&p, sig + 32 + p.l * p.polyz_packed, NULL, 0)) st |= 1;
     for (j = 0; j < p.l; j++) {
         unpack_offset(z, sig + 32 + j * p.polyz_packed, p.gamma1, z_bits(&p));
         if (chknorm(z, p.gamma1 - p.beta)) st |= 2;
@@ -614,31 +644,19 @@ int ora_sk_check(int mode, const uint8_t *sk) {
 
 /* ---------------------------------------------------------------- verify */
 
-int ora_verify(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen, const uint8_t *pk) {
+static int verify_impl(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen,
+                       const uint8_t *pk, int xor_lanes) {
     ora_params p;
     static __thread int32_t mat[MAXK * MAXL * N];
     int32_t z[MAXL][N], t1[MAXK][N], w1[MAXK][N], cp[N];
     uint8_t hint[MAXK][N];
     uint8_t trm[32], mu[64], w1packed[MAXK * 192], c2[32];
-    const uint8_t *hs;
     ora_xof st;
-    int i, j, c, kk;
+    int i, j, c;
     if (ora_params_get(mode, &p)) return -1;
     if (siglen != (size_t)p.sig_bytes) return -1;
     /* hint decode with the ordering / omega / zero-padding checks (src/verify.cu:51-93) */
-    hs = sig + 32 + p.l * p.polyz_packed;
-    memset(hint, 0, sizeof hint);
-    kk = 0;
-    for (i = 0; i < p.k; i++) {
-        if (hs[p.omega + i] < kk || hs[p.omega + i] > p.omega) return -1;
-        for (j = kk; j < hs[p.omega + i]; j++) {
-            if (j > kk && hs[j] <= hs[j - 1]) return -1;
-            hint[i][hs[j]] = 1;
-        }
-        kk = hs[p.omega + i];
-    }
-    for (j = kk; j < p.omega; j++)
-        if (hs[j]) return -1;
+    if (hint_decode(&p, sig + 32 + p.l * p.polyz_packed, hint, xor_lanes)) return -1;
     for (j = 0; j < p.l; j++) {
         unpack_offset(z[j], sig + 32 + j * p.polyz_packed, p.gamma1, z_bits(&p));
         if (chknorm(z[j], p.gamma1 - p.beta)) return -1;
@@ -679,6 +697,19 @@ int ora_verify(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, si
     for (i = 0; i < 32; i++)
         if (c2[i] != sig[i]) return -1;
     return 0;
+}
+
+/* Verification as the scheme states it: the checker for the CUDA library. */
+int ora_verify(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen, const uint8_t *pk) {
+    return verify_impl(mode, sig, siglen, m, mlen, pk, 0);
+}
+
+/* Verification with the reference kernel's XOR-combined hint-encoding ballots
+ * (src/verify.cu:66, :85; see hint_decode).  It accepts some non-canonical hint encodings of
+ * valid signatures that ora_verify and the CUDA library reject. */
+int ora_verify_xor_ballots(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen,
+                           const uint8_t *pk) {
+    return verify_impl(mode, sig, siglen, m, mlen, pk, 1);
 }
 
 /* ---------------------------------------------------------------- batches */

@@ -58,6 +58,9 @@ int ora_sign_rhoprime(int mode, uint8_t *sig, const uint8_t *m, size_t mlen, con
                       const uint8_t *rhoprime, int *attempts);
 int ora_verify(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen, const uint8_t *pk);
 int ora_sig_check(int mode, const uint8_t *sig);
+int ora_hint_check(int mode, const uint8_t *sig, int xor_lanes);
+int ora_verify_xor_ballots(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen,
+                           const uint8_t *pk);
 int ora_sk_check(int mode, const uint8_t *sk);
 
 /* Batched forms (OpenMP over items; nthreads <= 0 means all available). */

@@ -17,14 +17,21 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libref_fips202.so"
-REF_SRC = Path("/root/reference/src/fips202/fips202.c")
+
+
+def ref_root() -> Path | None:
+    """Root of the reference source tree, from CUDIL_REF_ROOT (unset: no reference build)."""
+    r = os.environ.get("CUDIL_REF_ROOT")
+    return Path(r) if r else None
 
 
 def build(ref: bool = True) -> None:
-    """make -C oracle (and the reference's own fips202.c into oracle/_ref when it is mounted)."""
+    """make -C oracle (and the reference's own fips202.c into oracle/_ref when CUDIL_REF_ROOT names
+    a reference tree that holds it)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    if ref and REF_SRC.exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    root = ref_root()
+    if ref and root is not None and (root / "src" / "fips202" / "fips202.c").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={root}"], check=True)
 
 
 class ora_params(ctypes.Structure):
@@ -46,6 +53,8 @@ def _load():
         "ora_sign": (c_int, [c_int, P8, P8, c_size_t, P8, POINTER(c_int)]),
         "ora_sign_rhoprime": (c_int, [c_int, P8, P8, c_size_t, P8, P8, POINTER(c_int)]),
         "ora_sig_check": (c_int, [c_int, P8]),
+        "ora_hint_check": (c_int, [c_int, P8, c_int]),
+        "ora_verify_xor_ballots": (c_int, [c_int, P8, c_size_t, P8, c_size_t, P8]),
         "ora_sk_check": (c_int, [c_int, P8]),
         "ora_verify": (c_int, [c_int, P8, c_size_t, P8, c_size_t, P8]),
         "ora_seed_from_ctr": (None, [P8, c_uint64]),
@@ -158,6 +167,22 @@ def sig_check(mode: int, sig: np.ndarray) -> np.ndarray:
     """Per-signature parse status: bit 0 bad hint encoding, bit 1 z out of range."""
     sig = np.ascontiguousarray(sig, dtype=np.uint8).reshape(-1, params(mode).sig_bytes)
     return np.array([lib.ora_sig_check(mode, _p(np.ascontiguousarray(r))) for r in sig], dtype=np.int32)
+
+
+def hint_check(mode: int, sig: np.ndarray, xor_lanes: bool = False) -> np.ndarray:
+    """Per-signature hint-encoding status (0 accepted, 1 rejected).  xor_lanes=True evaluates the
+    checks as the reference kernel does (lane ballots combined with XOR, src/verify.cu:66, :85)."""
+    sig = np.ascontiguousarray(sig, dtype=np.uint8).reshape(-1, params(mode).sig_bytes)
+    return np.array([lib.ora_hint_check(mode, _p(np.ascontiguousarray(r)), int(xor_lanes)) for r in sig],
+                    dtype=np.int32)
+
+
+def verify_xor_ballots(mode: int, sig: np.ndarray, m: bytes, pk: np.ndarray) -> int:
+    """One verification with the reference kernel's XOR-combined hint ballots (0 valid, -1 not)."""
+    s = np.ascontiguousarray(sig, dtype=np.uint8).reshape(-1)
+    mb = np.frombuffer(bytes(m) + b"\0", np.uint8)
+    k = np.ascontiguousarray(pk, dtype=np.uint8).reshape(-1)
+    return int(lib.ora_verify_xor_ballots(mode, _p(s), s.size, _p(mb), len(m), _p(k)))
 
 
 def sk_check(mode: int, sk: np.ndarray) -> np.ndarray:

@@ -29,10 +29,11 @@ def test_keccak_matches_reference_fips202(oracle):
     """Byte-for-byte against the reference's own src/fips202/fips202.c compiled into oracle/_ref."""
     import ctypes
     if not oracle.REF_LIB.exists():
-        if oracle.REF_SRC.exists():
+        root = oracle.ref_root()
+        if root is not None and (root / "src" / "fips202" / "fips202.c").exists():
             oracle.build(ref=True)
         else:
-            pytest.skip("reference fips202.c not available here")
+            pytest.skip("reference fips202.c not built (set CUDIL_REF_ROOT to the reference tree)")
     ref = ctypes.CDLL(str(oracle.REF_LIB))
     rng = random.Random(11)
     for n in [0, 3, 136, 168, 333, 2000]:
@@ -107,3 +108,25 @@ def test_oracle_parse_checks(oracle, mode):
     bsk = sk.copy()
     bsk[3, 96] = 0xFF
     assert oracle.sk_check(mode, bsk)[3] == 1
+
+
+def test_reference_xor_ballots_accept_noncanonical_hints(oracle):
+    """The reference's XOR-combined hint ballots (src/verify.cu:66, :85) accept re-encoded valid
+    signatures that the scheme's checks -- the oracle's ora_verify and the CUDA library -- reject.
+    This pins the one place where verification deliberately differs from the reference."""
+    from hint_cases import all_cases
+    for label, mode, pk, m, sig, bad in all_cases(oracle):
+        assert oracle.verify_batch(mode, sig[None], m[None], pk[None])[0] == 0, label
+        assert oracle.verify_xor_ballots(mode, sig, m.tobytes(), pk) == 0, label
+        # the re-encoding keeps the decoded hints: the reference's form still accepts it ...
+        assert oracle.verify_xor_ballots(mode, bad, m.tobytes(), pk) == 0, label
+        assert oracle.hint_check(mode, bad, xor_lanes=True)[0] == 0, label
+        # ... while the scheme's form rejects it
+        assert oracle.verify_batch(mode, bad[None], m[None], pk[None])[0] == -1, label
+        assert oracle.hint_check(mode, bad)[0] == 1 and oracle.sig_check(mode, bad)[0] & 1, label
+    # a single violation is rejected by both forms
+    pk, m, sig, bad = all_cases(oracle)[0][2:]
+    p = oracle.params(2)
+    one = bad.copy()
+    one[32 + p.l * p.polyz_packed + int(sig[32 + p.l * p.polyz_packed + p.omega + p.k - 1]) + 32] = 0
+    assert oracle.verify_xor_ballots(2, one, m.tobytes(), pk) == -1

@@ -30,14 +30,20 @@ def _batch(oracle, mode, n, mlen, seed):
     return sig, m, pk
 
 
-def _verify_noalloc(lib, torch, mode, sig, m, pk):
+def _stage(torch, sig, m, pk):
+    """Pinned host copies of a batch and a pinned result array (host memory only)."""
     from cudilithium_b200.api import pinned
-    n, mlen = m.shape
     hs, hm, hp = pinned(sig.size), pinned(max(m.size, 1)), pinned(pk.size)
     hs.numpy()[: sig.size] = sig.reshape(-1)
     hm.numpy()[: m.size] = m.reshape(-1)
     hp.numpy()[: pk.size] = pk.reshape(-1)
-    ret = torch.full((n,), 7, dtype=torch.int32, pin_memory=True)
+    ret = torch.full((m.shape[0],), 7, dtype=torch.int32, pin_memory=True)
+    return hs, hm, hp, ret
+
+
+def _call(lib, torch, mode, staged, sig, m):
+    hs, hm, hp, ret = staged
+    n, mlen = m.shape
     rc = lib.cudil_verify_noalloc(mode, ret.data_ptr(), hs.data_ptr(), sig.shape[1], sig.shape[1], hm.data_ptr(),
                                   mlen, mlen, hp.data_ptr(), n, None)
     assert rc == 0
@@ -54,8 +60,14 @@ def test_verify_noalloc_matches_verify_twice(cuda_ok, oracle, mode):
     d = Dilithium(mode)
     first = _batch(oracle, mode, 96, 32, seed=mode)
     second = _batch(oracle, mode, 61, 200, seed=mode + 40)
-    for sig, m, pk in (first, second):
-        got = _verify_noalloc(lib, torch, mode, sig, m, pk)
+    for k, (sig, m, pk) in enumerate((first, second)):
+        staged = _stage(torch, sig, m, pk)
+        # the first call may load the library's module (and its fixed array) on this device; from
+        # then on a call must not take any device memory
+        free0 = torch.cuda.mem_get_info()[0]
+        got = _call(lib, torch, mode, staged, sig, m)
+        if k:
+            assert torch.cuda.mem_get_info()[0] >= free0, "cudil_verify_noalloc took device memory"
         want = d.verify(sig, m, pk)
         assert np.array_equal(got, want)
         assert np.any(got == 0) and np.any(got == -1)
