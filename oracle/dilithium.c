@@ -146,7 +146,8 @@ static unsigned brv8(unsigned x) {
 
 /* zetas[i] = 2^32 * 1753^brv8(i) mod q, centred; zetas[0] is unused and kept 0 as in
  * src/ntt.cu:24. */
-static void zetas_init(void) {
+/* Run once at library load (see keccak_tables_init); later calls return at once. */
+__attribute__((constructor)) static void zetas_init(void) {
     int i;
     uint64_t mont = (1ULL << 32) % Q;
     if (g_zetas_ready) return;

@@ -36,7 +36,10 @@ static int rc_bit(unsigned t) {
     return r & 1;
 }
 
-static void keccak_tables_init(void) {
+/* Runs once when the library is loaded, before any caller can start threads: a lazy first-use
+ * initialisation raced when the first permutations ran on several OpenMP threads at once (a second
+ * initialiser cleared g_rot while a first thread was already permuting with it). */
+__attribute__((constructor)) static void keccak_tables_init(void) {
     unsigned ir, j, t, x, y;
     if (g_ready) return;
     for (ir = 0; ir < 24; ir++) {

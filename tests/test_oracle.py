@@ -130,3 +130,19 @@ def test_reference_xor_ballots_accept_noncanonical_hints(oracle):
     one = bad.copy()
     one[32 + p.l * p.polyz_packed + int(sig[32 + p.l * p.polyz_packed + p.omega + p.k - 1]) + 32] = 0
     assert oracle.verify_xor_ballots(2, one, m.tobytes(), pk) == -1
+
+
+def test_first_call_on_many_threads_is_deterministic():
+    """The oracle's tables are ready before any caller thread runs: a fresh process whose first
+    oracle call is a batch on several OpenMP threads gets the same keys as a single thread."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "import numpy as np\n"
+            "from oracle import pyoracle as O\n"
+            "pk, sk = O.keypair_batch(2, 512, 0, 8)\n"
+            "pk1, sk1 = O.keypair_seeds(2, O.seeds_from_ctr(512), 1)\n"
+            "assert np.array_equal(pk, pk1) and np.array_equal(sk, sk1)\n" % str(Path(__file__).resolve().parents[1]))
+    for _ in range(3):
+        subprocess.run([sys.executable, "-c", code], check=True)
