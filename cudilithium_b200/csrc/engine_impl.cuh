@@ -163,7 +163,7 @@ struct EngineImpl : EngineBase {
         if (rc) return rc;
         rc = configure_wide();
         if (rc) return rc;
-        prehash_grid = (int)std::min<size_t>((mi + kBlock - 1) / kBlock, (size_t)sm_count * 8);
+        prehash_grid = (int)std::min<size_t>((mi + kPrehashBlock - 1) / kPrehashBlock, (size_t)sm_count * 32);
         device_bytes = required_bytes(mk, mi);
         if (budget && device_bytes > budget) return CUDIL_ERR_BUDGET;
         sk_pitch = align256(C::SK_ROW);
@@ -340,7 +340,7 @@ struct EngineImpl : EngineBase {
                      unsigned spec) {
         MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order, d_rhop};
         k_fused_init<<<std::max(1, sm_count * 2), 256, 0, st>>>(q, best, locks, next_nonce, inflight);
-        k_fused_prehash<MODE><<<prehash_grid, kBlock, 0, st>>>(sk_cache, sk_pitch, mr, items, q);
+        k_fused_prehash<MODE><<<prehash_grid, kPrehashBlock, 0, st>>>(sk_cache, sk_pitch, mr, items, q);
         FusedSignArgs a{sk_cache, sk_pitch, d_key, items, d_sig, (size_t)PM::SIG_BYTES, scratch, q, best, locks, next_nonce,
                         inflight, spec, nonce_limit, lock_spins, idle_polls};
         if (variant == 1)

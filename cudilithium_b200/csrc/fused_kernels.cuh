@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(kBlock) k_cache_pk_tr(const uint8_t *pk, uint8
         const uint8_t *p;
         __device__ uint2 lane(long long g) const { return load_lane_bytes(p + g * 8, (int)(PM::PK_BYTES - g * 8)); }
     } src{p};
-    shake_absorb<SHAKE256_RATE>(al, ah, src, PM::PK_BYTES);
+    shake_absorb_prefetch<SHAKE256_RATE>(al, ah, src, PM::PK_BYTES);
     keccak_f1600(al, ah);
     uint2 *tr = reinterpret_cast<uint2 *>(row + C::PK_TR);
 #pragma unroll
@@ -182,9 +182,13 @@ struct MsgRefs {
     const uint8_t *rhoprime;  // randomized signing: 64 bytes per item (dense); nullptr = SHAKE256(K || mu)
 };
 
+// One warp per block, so that the warps holding the longest messages (the order is longest first)
+// spread over all SMs.
+constexpr int kPrehashBlock = 32;
+
 template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_fused_prehash(const uint8_t *cache, size_t cpitch, MsgRefs mr, uint8_t *items,
-                                                          const FusedQueue *q) {
+__global__ void __launch_bounds__(kPrehashBlock) k_fused_prehash(const uint8_t *cache, size_t cpitch, MsgRefs mr,
+                                                                 uint8_t *items, const FusedQueue *q) {
     using C = Cache<MODE>;
     const unsigned n = q->n;
     for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -192,7 +196,7 @@ __global__ void __launch_bounds__(kBlock) k_fused_prehash(const uint8_t *cache, 
         const uint8_t *row = cache + (size_t)mr.key_idx[it] * cpitch;
         uint32_t al[25], ah[25];
         TwoPart src{row + C::SK_TR, 4, mr.msgs + mr.offsets[it], (long long)mr.mlens[it]};
-        shake_absorb<SHAKE256_RATE>(al, ah, src, (long long)SEEDBYTES + mr.mlens[it]);
+        shake_absorb_prefetch<SHAKE256_RATE>(al, ah, src, (long long)SEEDBYTES + mr.mlens[it]);
         keccak_f1600(al, ah);
         uint2 mu[8];
 #pragma unroll

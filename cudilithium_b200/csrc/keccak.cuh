@@ -203,6 +203,54 @@ __device__ __forceinline__ void shake_absorb(uint32_t (&al)[25], uint32_t (&ah)[
     }
 }
 
+// shake_absorb for long inputs read from global memory: the next block's lanes are loaded before
+// the current block is permuted, so their latency overlaps the permutation instead of preceding
+// the next one (RATE / 4 more registers live across the permutation; for kernels whose register
+// budget allows it, such as the message hashes of the prehash kernels).
+template <int RATE, typename Src>
+__device__ __forceinline__ void shake_absorb_prefetch(uint32_t (&al)[25], uint32_t (&ah)[25], const Src &src,
+                                                      long long total_bytes) {
+    constexpr int RL = RATE / 8;
+    keccak_zero(al, ah);
+    const long long nfull = total_bytes / RATE;
+    uint2 nxt[RL];
+    if (nfull > 0) {
+#pragma unroll
+        for (int w = 0; w < RL; ++w) nxt[w] = src.lane(w);
+    }
+    long long g = 0;
+#pragma unroll 1
+    for (long long blk = 0; blk < nfull; ++blk) {
+#pragma unroll
+        for (int w = 0; w < RL; ++w) {
+            al[w] ^= nxt[w].x;
+            ah[w] ^= nxt[w].y;
+        }
+        g += RL;
+        if (blk + 1 < nfull) {
+#pragma unroll
+            for (int w = 0; w < RL; ++w) nxt[w] = src.lane(g + w);
+        }
+        keccak_f1600(al, ah);
+    }
+    const int rem = (int)(total_bytes - nfull * RATE);
+#pragma unroll
+    for (int w = 0; w < RL; ++w) {
+        uint2 v = make_uint2(0u, 0u);
+        if (8 * w < rem) v = src.lane(g + w);
+        if (8 * w <= rem && rem < 8 * w + 8) {
+            const int sh = 8 * (rem - 8 * w);
+            if (sh < 32)
+                v.x ^= 0x1Fu << sh;
+            else
+                v.y ^= 0x1Fu << (sh - 32);
+        }
+        if (w == RL - 1) v.y ^= 0x80000000u;
+        al[w] ^= v.x;
+        ah[w] ^= v.y;
+    }
+}
+
 // Absorb of a short input of IN_LANES whole lanes plus an extra 16-bit little-endian nonce
 // (seed || nonce, as ExpandA/ExpandS/ExpandMask use); the input must fit one block.
 template <int RATE, int IN_LANES>

@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kBlock) k_kp_tr(uint8_t *pool, size_t pitch, i
     uint8_t *row = pool + (size_t)it * pitch;
     uint32_t al[25], ah[25];
     AlignedBytes pk{row + LY::KP_PK, PM::PK_BYTES};
-    shake_absorb<SHAKE256_RATE>(al, ah, pk, PM::PK_BYTES);
+    shake_absorb_prefetch<SHAKE256_RATE>(al, ah, pk, PM::PK_BYTES);
     keccak_f1600(al, ah);
     uint2 *tr = reinterpret_cast<uint2 *>(row + LY::KP_SK + PM::SK_TR);
 #pragma unroll

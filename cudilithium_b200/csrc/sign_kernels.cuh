@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_prehash(uint8_t *pool, size_t p
     const size_t ml = mlens ? (size_t)mlens[it] : mlen;  // per-item length (<= mlen) when given
     uint32_t al[25], ah[25];
     TwoPart src{row + LY::SG_SK + P<MODE>::SK_TR, 4, row + LY::SG_MSG, (long long)ml};
-    shake_absorb<SHAKE256_RATE>(al, ah, src, (long long)(SEEDBYTES + ml));
+    shake_absorb_prefetch<SHAKE256_RATE>(al, ah, src, (long long)(SEEDBYTES + ml));
     keccak_f1600(al, ah);
     uint2 mu[8];
 #pragma unroll

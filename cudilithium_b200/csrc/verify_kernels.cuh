@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(TB) k_verify_prepare(uint8_t *pool, size_t pit
     uint32_t al[25], ah[25];
     // tr' = SHAKE256(pk, 32) -> row + VF_TRM (m follows it)
     AlignedBytes pk{row + LY::VF_PK, PM::PK_BYTES};
-    shake_absorb<SHAKE256_RATE>(al, ah, pk, PM::PK_BYTES);
+    shake_absorb_prefetch<SHAKE256_RATE>(al, ah, pk, PM::PK_BYTES);
     keccak_f1600(al, ah);
     uint2 *trm = reinterpret_cast<uint2 *>(row + LY::VF_TRM);
 #pragma unroll
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(TB) k_verify_prepare(uint8_t *pool, size_t pit
     // mu = SHAKE256(tr' || m, 64); per-item length (<= mlen) when given
     const size_t ml = mlens ? (size_t)mlens[it] : mlen;
     AlignedBytes tm{row + LY::VF_TRM, (long long)(SEEDBYTES + ml)};
-    shake_absorb<SHAKE256_RATE>(al, ah, tm, (long long)(SEEDBYTES + ml));
+    shake_absorb_prefetch<SHAKE256_RATE>(al, ah, tm, (long long)(SEEDBYTES + ml));
     keccak_f1600(al, ah);
     uint2 *mu = reinterpret_cast<uint2 *>(row + LY::vf_mu(mlen));
 #pragma unroll
