@@ -6,10 +6,14 @@ module raises, so nothing can silently run on the CPU.
 from __future__ import annotations
 
 import ctypes
+import os
 from ctypes import POINTER, c_char_p, c_int, c_int32, c_size_t, c_uint8, c_uint16, c_uint32, c_void_p
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libcudilithium_b200.so"
+# CUDIL_LIB selects another build of the library (for example the bounds-checked
+# libcudilithium_b200_bc.so); default: the in-tree libcudilithium_b200.so
+LIB_PATH = (Path(os.environ["CUDIL_LIB"]) if os.environ.get("CUDIL_LIB")
+            else Path(__file__).resolve().parent / "libcudilithium_b200.so")
 
 CUDIL_OK = 0
 CUDIL_ERR_INVALID = -1
@@ -132,6 +136,10 @@ SIGNATURES = {
     "cudil_engine_set_spec_slots": (c_int, [c_void_p, c_uint32]),
     "cudil_engine_set_sign_kernel": (c_int, [c_void_p, c_int]),
     "cudil_engine_set_limits": (c_int, [c_void_p, c_uint32, c_uint32, c_uint32]),
+    "cudil_engine_sign_seeded": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p,
+                                         c_void_p, ctypes.c_ulonglong, c_size_t, c_void_p]),
+    "cudil_derive_rhoprime": (c_int, [c_void_p, c_size_t, c_void_p, ctypes.c_ulonglong, c_size_t, c_void_p]),
+    "cudil_bounds_check_status": (c_int, [POINTER(c_uint32), c_int]),
     "cudil_engine_last_nonces": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
     "cudil_engine_set_large_batch": (c_int, [c_void_p, c_size_t, c_int, c_uint32]),
     "cudil_engine_last_jobs": (c_int, [c_void_p, POINTER(ctypes.c_ulonglong)]),

@@ -262,6 +262,17 @@ class Dilithium:
         return ret.numpy()[:n].copy()
 
 
+def derive_rhoprime(seed: bytes, counter: int, n: int, stream=None) -> torch.Tensor:
+    """(n, 64) uint8 CUDA tensor of randomized-signing seeds, row i = SHAKE256(seed || le64(counter + i),
+    64), derived on the device from one 32-byte seed (cudil_derive_rhoprime)."""
+    seed = bytes(seed)
+    if len(seed) != 32:
+        raise ValueError("seed must be 32 bytes")
+    out = torch.empty((max(n, 1), 64), dtype=torch.uint8, device="cuda")
+    check(lib.cudil_derive_rhoprime(_ptr(out), 64, seed, counter, n, _stream_ptr(stream)), "cudil_derive_rhoprime")
+    return out[:n]
+
+
 def ntt_mul(a: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
     """out[p] = invNTT(NTT(a[p]) o b[p]) for int32 CUDA tensors of shape (npolys, 256)."""
     assert a.is_cuda and b.is_cuda and a.dtype == torch.int32 and b.dtype == torch.int32

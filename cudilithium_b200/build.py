@@ -19,6 +19,8 @@ CSRC = PKG / "csrc"
 ROOT = PKG.parent
 LIB = PKG / "libcudilithium_b200.so"
 OBJ_DIR = PKG / "_build"
+LIB_BC = PKG / "libcudilithium_b200_bc.so"
+OBJ_DIR_BC = PKG / "_build_bc"
 
 NVCC_FLAGS = [
     "-O3",
@@ -50,19 +52,24 @@ def _stale(obj: Path, src: Path) -> bool:
     return any(d.stat().st_mtime > t for d in deps if d.exists())
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
+def build(verbose: bool = False, force: bool = False, bounds_check: bool = False) -> Path:
+    """Compiles and links the library; bounds_check=True makes the bounds-checked variant
+    libcudilithium_b200_bc.so (device-side range checks, -DCUDIL_BOUNDS_CHECK) beside it."""
     nvcc = _nvcc()
-    OBJ_DIR.mkdir(exist_ok=True)
+    obj_dir = OBJ_DIR_BC if bounds_check else OBJ_DIR
+    lib = LIB_BC if bounds_check else LIB
+    flags = NVCC_FLAGS + (["-DCUDIL_BOUNDS_CHECK"] if bounds_check else [])
+    obj_dir.mkdir(exist_ok=True)
     srcs = sources()
     jobs = []
     for s in srcs:
-        o = OBJ_DIR / (s.stem + ".o")
+        o = obj_dir / (s.stem + ".o")
         if force or _stale(o, s):
             jobs.append((s, o))
 
     def run(job):
         s, o = job
-        cmd = [nvcc, *NVCC_FLAGS, "-c", str(s), "-o", str(o)]
+        cmd = [nvcc, *flags, "-c", str(s), "-o", str(o)]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -72,18 +79,17 @@ def build(verbose: bool = False, force: bool = False) -> Path:
 
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 4))) as ex:
         list(ex.map(run, jobs))
-    objs = [OBJ_DIR / (s.stem + ".o") for s in srcs]
-    if force or jobs or not LIB.exists():
-        cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(LIB), *map(str, objs),
+    objs = [obj_dir / (s.stem + ".o") for s in srcs]
+    if force or jobs or not lib.exists():
+        cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(lib), *map(str, objs),
                "-cudart", "static"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv, force="-f" in sys.argv)
-    print(LIB)
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv, bounds_check="--bounds-check" in sys.argv))

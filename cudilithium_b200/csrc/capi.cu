@@ -14,6 +14,9 @@ namespace cudil {
 extern template struct Impl<2>;
 extern template struct Impl<3>;
 extern template struct Impl<5>;
+cudaError_t bounds_status_mode2(unsigned *out, bool reset);
+cudaError_t bounds_status_mode3(unsigned *out, bool reset);
+cudaError_t bounds_status_mode5(unsigned *out, bool reset);
 
 // Peak of the 32-bit logic/shift mix that Keccak-f[1600] issues (3 LOP3 : 1 funnel shift, the
 // ratio of a LOP3/SHF lowering of theta/rho/chi): 8 independent chains per thread.
@@ -37,6 +40,30 @@ __global__ void __launch_bounds__(256) k_alu_peak(uint32_t *out, int iters) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) r ^= a[k];
     out[blockIdx.x * blockDim.x + threadIdx.x] = r;
+}
+
+// Seeded randomized signing: row i of out (pitch bytes apart) = SHAKE256(seed || le64(counter + i),
+// 64), one thread per row; the seed travels by value in the kernel arguments.
+struct Seed32 {
+    uint32_t w[8];
+};
+
+__global__ void __launch_bounds__(kBlock) k_derive_rhoprime(uint8_t *out, size_t pitch, Seed32 seed,
+                                                            unsigned long long counter, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint2 rp[8];
+    derive_rhoprime(rp, seed.w, counter + (unsigned long long)i);
+    uint8_t *row = out + (size_t)i * pitch;
+    if ((reinterpret_cast<uintptr_t>(row) & 7u) == 0u) {
+#pragma unroll
+        for (int w = 0; w < 8; ++w) reinterpret_cast<uint2 *>(row)[w] = rp[w];
+    } else {
+#pragma unroll
+        for (int w = 0; w < 8; ++w)
+#pragma unroll
+            for (int b = 0; b < 8; ++b) row[8 * w + b] = (uint8_t)((b < 4 ? rp[w].x >> (8 * b) : rp[w].y >> (8 * (b - 4))));
+    }
 }
 
 // out = invNTT(NTT(a) o b) for npolys polynomial pairs.  A grid of a few blocks per SM walks the
@@ -358,6 +385,34 @@ int cudil_ntt_mul(const int32_t *d_a, const int32_t *d_b, int32_t *d_out, size_t
     const unsigned grid = (unsigned)(need < (size_t)blocks ? need : (size_t)blocks);
     CUDIL_LAUNCH(KID_NTT_MUL, st, k_ntt_mul<<<grid, kBlock, 0, st>>>(d_a, d_b, d_out, (long long)npolys));
     return cudaGetLastError() == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
+}
+
+int cudil_derive_rhoprime(uint8_t *d_rhoprime, size_t rhoprime_pitch, const uint8_t *seed, unsigned long long counter,
+                          size_t n, void *stream) {
+    if (n == 0) return CUDIL_OK;
+    if (!d_rhoprime || !seed || rhoprime_pitch < 64 || n > (size_t)LLONG_MAX / rhoprime_pitch) return CUDIL_ERR_INVALID;
+    Seed32 s;
+    std::memcpy(s.w, seed, sizeof s.w);
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned blocks = (unsigned)((n + kBlock - 1) / kBlock);
+    CUDIL_LAUNCH(KID_DERIVE_RHOP, st,
+                 k_derive_rhoprime<<<blocks, kBlock, 0, st>>>(d_rhoprime, rhoprime_pitch, s, counter, (long long)n));
+    return cudaGetLastError() == cudaSuccess ? CUDIL_OK : CUDIL_ERR_CUDA;
+}
+
+int cudil_bounds_check_status(unsigned *error, int reset) {
+    if (!error) return CUDIL_ERR_INVALID;
+    *error = 0;
+    if (!kBoundsChecked) return CUDIL_ERR_INVALID;
+    cudaError_t (*const words[])(unsigned *, bool) = {bounds_status_mode2, bounds_status_mode3, bounds_status_mode5,
+                                                      bounds_status_here};
+    for (auto fn : words) {
+        unsigned v = 0;
+        const cudaError_t e = fn(&v, reset != 0);
+        if (e != cudaSuccess) return cudil_record_cuda_error(e, __FILE__, __LINE__);
+        if (!*error) *error = v;
+    }
+    return CUDIL_OK;
 }
 
 int cudil_alu_peak(uint32_t *d_out, int blocks, int iters, void *stream, double *ops_per_launch) {

@@ -5,6 +5,7 @@
 #include <cstdint>
 
 #include "arith.cuh"
+#include "bounds.cuh"
 #include "keccak.cuh"
 #include "ntt.cuh"
 #include "params.cuh"

@@ -110,6 +110,14 @@ int cudil_engine_sign_randomized(cudil_engine *e, uint8_t *d_sig, const uint8_t 
     CUDIL_ENGINE_DISPATCH(e, sign(d_sig, d_msgs, msgs_bytes, offsets, mlens, key_idx, n, (cudaStream_t)stream, d_rhoprime));
 }
 
+int cudil_engine_sign_seeded(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
+                             const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx,
+                             const uint8_t *rho_seed, unsigned long long rho_counter, size_t n, void *stream) {
+    if (!rho_seed && n) return CUDIL_ERR_INVALID;
+    CUDIL_ENGINE_DISPATCH(e, sign(d_sig, d_msgs, msgs_bytes, offsets, mlens, key_idx, n, (cudaStream_t)stream, nullptr,
+                                  rho_seed, rho_counter));
+}
+
 int cudil_engine_verify(cudil_engine *e, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
                         const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
                         void *stream) {

@@ -302,7 +302,8 @@ struct EngineImpl : EngineBase {
 
     // ------------------------------------------------------------ metadata upload
     int upload_meta(const unsigned long long *off, const unsigned *mlen, const unsigned *key, size_t n, size_t nkeys,
-                    size_t msgs_bytes, bool longest_first, cudaStream_t st) {
+                    size_t msgs_bytes, bool longest_first, cudaStream_t st, const uint8_t *rho_seed = nullptr,
+                    unsigned long long rho_counter = 0) {
         // the previous batch's copies out of the staging buffer must have completed (only those:
         // work the caller queued on the stream, such as input copies or cache builds, keeps
         // running while this batch is prepared)
@@ -310,6 +311,11 @@ struct EngineImpl : EngineBase {
         FusedQueue *hq = reinterpret_cast<FusedQueue *>(h_stage);
         std::memset(hq, 0, sizeof(FusedQueue));
         hq->n = (unsigned)n;
+        if (rho_seed) {
+            hq->rho_seeded = 1u;
+            hq->rho_counter = rho_counter;
+            std::memcpy(hq->rho_seed, rho_seed, sizeof hq->rho_seed);
+        }
         unsigned *hk = reinterpret_cast<unsigned *>(h_stage + kStageHead);
         unsigned *hm = hk + max_items;
         unsigned *ho = hm + max_items;
@@ -338,11 +344,11 @@ struct EngineImpl : EngineBase {
     template <int T>
     void record_sign(cudaStream_t st, uint8_t *d_sig, const uint8_t *d_msgs, const uint8_t *d_rhop, int variant,
                      unsigned spec) {
-        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order, d_rhop};
+        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order, d_rhop, (unsigned)max_keys};
         k_fused_init<<<std::max(1, sm_count * 2), 256, 0, st>>>(q, best, locks, next_nonce, inflight);
         k_fused_prehash<MODE><<<prehash_grid, kPrehashBlock, 0, st>>>(sk_cache, sk_pitch, mr, items, q);
         FusedSignArgs a{sk_cache, sk_pitch, d_key, items, d_sig, (size_t)PM::SIG_BYTES, scratch, q, best, locks, next_nonce,
-                        inflight, spec, nonce_limit, lock_spins, idle_polls};
+                        inflight, spec, nonce_limit, lock_spins, idle_polls, (unsigned)max_keys};
         if (variant == 1)
             k_fused_sign_async<MODE, 256, 64><<<async_grid[0], 256, async_smem[0], st>>>(a);
         else if (variant == 2)
@@ -360,7 +366,7 @@ struct EngineImpl : EngineBase {
 
     template <int T>
     void record_verify(cudaStream_t st, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs) {
-        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order, nullptr};
+        MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order, nullptr, (unsigned)max_keys};
         k_fused_init<<<1, 32, 0, st>>>(q, best, locks, nullptr, nullptr);
         k_fused_verify<MODE, T><<<verify_grid, T, verify_smem, st>>>(pk_cache, pk_pitch, mr, d_sig, PM::SIG_BYTES, d_ret,
                                                                     scratch, q);
@@ -393,8 +399,11 @@ struct EngineImpl : EngineBase {
     }
 
     // d_rhop: randomized signing seeds, 64 bytes per item (dense, device); nullptr = deterministic
+    // rho_seed (host, 32 bytes): seeded randomized signing, rho' of item i derived on the device from
+    // (rho_seed, rho_counter + i); it goes up with the batch metadata, so the graph is unchanged
     int sign(uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes, const unsigned long long *off, const unsigned *mlen,
-             const unsigned *key, size_t n, cudaStream_t st, const uint8_t *d_rhop = nullptr) {
+             const unsigned *key, size_t n, cudaStream_t st, const uint8_t *d_rhop = nullptr,
+             const uint8_t *rho_seed = nullptr, unsigned long long rho_counter = 0) {
         if (n == 0) return CUDIL_OK;
         if (!d_sig || !off || !mlen || !key || n > max_items || n_sk == 0) return CUDIL_ERR_INVALID;
         if (!d_msgs) {
@@ -422,7 +431,7 @@ struct EngineImpl : EngineBase {
                 out = static_cast<uint8_t *>(pa.devicePointer);
             }
         }
-        int rc = upload_meta(off, mlen, key, n, n_sk, msgs_bytes, true, st);
+        int rc = upload_meta(off, mlen, key, n, n_sk, msgs_bytes, true, st, rho_seed, rho_counter);
         if (rc) return rc;
         if (recapture) {
             // for a signing graph the `sig` argument of capture carries the randomized-signing seeds

@@ -77,6 +77,12 @@ struct FusedQueue {
     // asynchronous signer, summed over warps: cycles in reject / w / challenge / ExpandMask / claim /
     // idle polls, then the number of each
     unsigned long long jobs[12];
+    // seeded randomized signing (set per batch by the host): rho' of item i is
+    // SHAKE256(rho_seed || le64(rho_counter + i), 64); rho_seeded = 0 keeps the other rho' sources
+    unsigned long long rho_counter;
+    unsigned rho_seeded;
+    unsigned pad3;
+    uint32_t rho_seed[8];
 };
 
 // ------------------------------------------------------------------ cache builders
@@ -180,6 +186,7 @@ struct MsgRefs {
     const unsigned int *key_idx;
     const unsigned int *order;
     const uint8_t *rhoprime;  // randomized signing: 64 bytes per item (dense); nullptr = SHAKE256(K || mu)
+    unsigned nkeys;           // key-cache rows allocated (bound of key_idx[])
 };
 
 // One warp per block, so that the warps holding the longest messages (the order is longest first)
@@ -193,6 +200,7 @@ __global__ void __launch_bounds__(kPrehashBlock) k_fused_prehash(const uint8_t *
     const unsigned n = q->n;
     for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         const unsigned it = mr.order[r];
+        if (!bc_ok(it < n && mr.key_idx[it] < mr.nkeys, BC_PREHASH_ITEM)) continue;
         const uint8_t *row = cache + (size_t)mr.key_idx[it] * cpitch;
         uint32_t al[25], ah[25];
         TwoPart src{row + C::SK_TR, 4, mr.msgs + mr.offsets[it], (long long)mr.mlens[it]};
@@ -204,6 +212,16 @@ __global__ void __launch_bounds__(kPrehashBlock) k_fused_prehash(const uint8_t *
         uint2 *out = reinterpret_cast<uint2 *>(items + (size_t)it * C::ITEM_BYTES);
 #pragma unroll
         for (int w = 0; w < 8; ++w) out[w] = mu[w];
+        if (q->rho_seeded) {
+            uint32_t seed[8];
+#pragma unroll
+            for (int w = 0; w < 8; ++w) seed[w] = q->rho_seed[w];
+            uint2 rp[8];
+            derive_rhoprime(rp, seed, q->rho_counter + it);
+#pragma unroll
+            for (int w = 0; w < 8; ++w) out[8 + w] = rp[w];
+            continue;
+        }
         if (mr.rhoprime) {
             const uint8_t *rp = mr.rhoprime + (size_t)it * CRHBYTES;
 #pragma unroll 1
@@ -281,6 +299,7 @@ struct FusedSignArgs {
     unsigned nonce_limit;  // nonces an item may use (the 16-bit nonce field allows 65536)
     unsigned lock_spins;   // tries for a per-item publication lock before giving up (error bit 0)
     unsigned idle_polls;   // empty polls before an asynchronous signer block gives up (error bit 2)
+    unsigned nkeys;        // key-cache rows allocated (bound of key_idx[])
 };
 
 // Sentinel best nonce of an item that used all its nonces without an accepted attempt: below the
@@ -457,34 +476,37 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
             if ((int)base >= total) break;
             const int job = (int)base + lane;
             // attempts above an already accepted nonce of their item are skipped (they cannot win)
-            if (job < na_c && __ldcg(arg.best + s_item[cb * A + job]) < s_nonce[cb * A + job]) {
-            } else if (job < na_c) {
-                const unsigned item = s_item[cb * A + job];
-                uint8_t *slot = slot_of(cb, job);
-                uint32_t al[25], ah[25];
-                TwoPart src{arg.items + (size_t)item * C::ITEM_BYTES, 8, slot + C::SL_W1P, PM::W1PACKED_BYTES};
-                shake_absorb<SHAKE256_RATE>(al, ah, src, CRHBYTES + PM::W1PACKED_BYTES);
-                keccak_f1600(al, ah);
-                uint2 ct[4];
+            if (job < na_c) {
+                const unsigned item = bc_ok(job < A, BC_SIGN_SLOT) ? s_item[cb * A + job] : 0xFFFFFFFFu;
+                if (bc_ok(item < n, BC_SIGN_SLOT) && !(__ldcg(arg.best + item) < s_nonce[cb * A + job])) {
+                    uint8_t *slot = slot_of(cb, job);
+                    uint32_t al[25], ah[25];
+                    TwoPart src{arg.items + (size_t)item * C::ITEM_BYTES, 8, slot + C::SL_W1P, PM::W1PACKED_BYTES};
+                    shake_absorb<SHAKE256_RATE>(al, ah, src, CRHBYTES + PM::W1PACKED_BYTES);
+                    keccak_f1600(al, ah);
+                    uint2 ct[4];
 #pragma unroll
-                for (int w = 0; w < 4; ++w) ct[w] = make_uint2(al[w], ah[w]);
-                uint2 *sg = reinterpret_cast<uint2 *>(slot + C::SL_SIG);
+                    for (int w = 0; w < 4; ++w) ct[w] = make_uint2(al[w], ah[w]);
+                    uint2 *sg = reinterpret_cast<uint2 *>(slot + C::SL_SIG);
 #pragma unroll
-                for (int w = 0; w < 4; ++w) sg[w] = ct[w];
-                sample_in_ball<PM::TAU, THREADS>(ct, blkw, mask);
-                uint4 *mo = reinterpret_cast<uint4 *>(slot + C::SL_CM);
+                    for (int w = 0; w < 4; ++w) sg[w] = ct[w];
+                    sample_in_ball<PM::TAU, THREADS>(ct, blkw, mask);
+                    uint4 *mo = reinterpret_cast<uint4 *>(slot + C::SL_CM);
 #pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    mo[k] = make_uint4(mask[(4 * k) * THREADS], mask[(4 * k + 1) * THREADS], mask[(4 * k + 2) * THREADS],
-                                       mask[(4 * k + 3) * THREADS]);
-            } else if (job < total && __ldcg(arg.best + s_item[nb * A + (job - na_c) / L]) < s_nonce[nb * A + (job - na_c) / L]) {
+                    for (int k = 0; k < 4; ++k)
+                        mo[k] = make_uint4(mask[(4 * k) * THREADS], mask[(4 * k + 1) * THREADS], mask[(4 * k + 2) * THREADS],
+                                           mask[(4 * k + 3) * THREADS]);
+                }
             } else if (job < total) {
                 const int idx = job - na_c, a = idx / L, j = idx % L;
-                const unsigned item = s_item[nb * A + a], nonce = s_nonce[nb * A + a];
-                uint2 rhop[8];
-                ld_lanes(rhop, arg.items + (size_t)item * C::ITEM_BYTES + 64);
-                expand_mask_stream<MODE>(slot_of(nb, a) + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, rhop,
-                                         (uint32_t)(L * nonce + j));
+                const bool slot_ok = bc_ok(a < A, BC_SIGN_SLOT);
+                const unsigned item = slot_ok ? s_item[nb * A + a] : 0xFFFFFFFFu, nonce = slot_ok ? s_nonce[nb * A + a] : 0u;
+                if (bc_ok(item < n, BC_SIGN_SLOT) && !(__ldcg(arg.best + item) < nonce)) {
+                    uint2 rhop[8];
+                    ld_lanes(rhop, arg.items + (size_t)item * C::ITEM_BYTES + 64);
+                    expand_mask_stream<MODE>(slot_of(nb, a) + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, rhop,
+                                             (uint32_t)(L * nonce + j));
+                }
             }
             __syncwarp();  // every lane runs the same grab / sync sequence
         }
@@ -492,16 +514,20 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
 
     // rejection checks, hints and publication of one attempt (group-collective)
     auto reject_job = [&](int cb, int a) {
+        // (range checks of the bounds-checked build: every value is the same across the group)
+        if (!bc_ok(a < A, BC_SIGN_SLOT)) return;
         const unsigned item = s_item[cb * A + a], nonce = s_nonce[cb * A + a];
+        if (!bc_ok(item < n, BC_SIGN_SLOT)) return;
         // one decision per group: out-of-range nonce, or a smaller nonce of the item already accepted
         bool skip = nonce > 0xFFFFu || __ldcg(arg.best + item) < nonce;
         skip = __shfl_sync(g.gmask, skip, lane_off);
-        if (skip) {
+        const unsigned key = arg.key_idx[item];
+        if (skip || !bc_ok(key < arg.nkeys, BC_SIGN_KEY)) {
             if (g.t == 0) atomicSub(arg.inflight + item, 1u);
             return;
         }
         uint8_t *slot = slot_of(cb, a);
-        const uint8_t *row = arg.cache + (size_t)arg.key_idx[item] * arg.cpitch;
+        const uint8_t *row = arg.cache + (size_t)key * arg.cpitch;
         g.sm = reinterpret_cast<int32_t *>(ph) + (size_t)gi * (L * N + NTT_SMEM_WORDS) + L * N;
         uint32_t masks[16];
         {
@@ -667,12 +693,15 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
 
     // w = invNTT(A_hat * NTT(y)), Decompose, pack w1 of one attempt (group-collective)
     auto w_job = [&](int nb, int a) {
+        if (!bc_ok(a < A, BC_SIGN_SLOT)) return;
         const unsigned item = s_item[nb * A + a];
+        if (!bc_ok(item < n, BC_SIGN_SLOT)) return;
         bool skip = __ldcg(arg.best + item) < s_nonce[nb * A + a];
         skip = __shfl_sync(g.gmask, skip, lane_off);
-        if (skip) return;
+        const unsigned key = arg.key_idx[item];
+        if (skip || !bc_ok(key < arg.nkeys, BC_SIGN_KEY)) return;
         uint8_t *slot = slot_of(nb, a);
-        const uint8_t *row = arg.cache + (size_t)arg.key_idx[item] * arg.cpitch;
+        const uint8_t *row = arg.cache + (size_t)key * arg.cpitch;
         int32_t *yh = reinterpret_cast<int32_t *>(ph) + (size_t)gi * (L * N + NTT_SMEM_WORDS);
         g.sm = yh + L * N;
 #pragma unroll 1
@@ -829,9 +858,11 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
         if (tid < na) {
             const unsigned it = base + tid;
             const uint8_t *s = sig + (size_t)it * sig_pitch;
-            const uint8_t *row = cache + (size_t)mr.key_idx[it] * cpitch;
+            const unsigned key = mr.key_idx[it];
+            const bool key_ok = bc_ok(key < mr.nkeys, BC_VERIFY_KEY);
+            const uint8_t *row = cache + (size_t)(key_ok ? key : 0u) * cpitch;
             uint8_t *slot = my_slots + (size_t)tid * C::VSLOT;
-            int status = 0;
+            int status = key_ok ? 0 : 4;
             const uint8_t *h = s + PM::SIG_H;
             int k = 0;
             for (int i = 0; i < K && !status; ++i) {
@@ -880,7 +911,8 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
             for (int a = gi; a < na; a += G) {
                 const unsigned it = base + a;
                 const uint8_t *s = sig + (size_t)it * sig_pitch;
-                const uint8_t *row = cache + (size_t)mr.key_idx[it] * cpitch;
+                const unsigned key = mr.key_idx[it];
+                const uint8_t *row = cache + (size_t)(bc_ok(key < mr.nkeys, BC_VERIFY_KEY) ? key : 0u) * cpitch;
                 uint8_t *slot = my_slots + (size_t)a * C::VSLOT;
                 bool zbad = false;
 #pragma unroll 1

@@ -211,6 +211,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
         if (act) {
             item = s_item[s];
             nonce = s_nonce[s];
+            act = bc_ok(item < n, BC_SIGN_SLOT);
         }
         const bool drop = act && superseded(item, nonce);
         if (act && !drop) {
@@ -242,9 +243,25 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
         __syncwarp();
     };
 
+    // bounds-checked build: a slot whose item or key index is out of range is dropped (warp-uniform)
+    auto bad_slot = [&](unsigned s, unsigned item) -> bool {
+        if (!bc_ok(item < n, BC_SIGN_SLOT)) {
+            if (lane == 0) publish(s, AS_FREE);
+            __syncwarp();
+            return true;
+        }
+        if (!bc_ok(arg.key_idx[item] < arg.nkeys, BC_SIGN_KEY)) {
+            if (lane == 0) retire(s, item);
+            __syncwarp();
+            return true;
+        }
+        return false;
+    };
+
     // ---------------------------------------------------------------- w = A y (warp per attempt)
     auto w_job = [&](unsigned s) {
         const unsigned item = s_item[s], nonce = s_nonce[s];
+        if (bad_slot(s, item)) return;
         if (superseded(item, nonce)) {
             if (lane == 0) retire(s, item);
             __syncwarp();
@@ -322,6 +339,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512) ? 1 : 512 / THREADS)
     // ---------------------------------------------------------------- rejection (warp per attempt)
     auto reject_job = [&](unsigned s) {
         const unsigned item = s_item[s], nonce = s_nonce[s];
+        if (bad_slot(s, item)) return;
         if (superseded(item, nonce)) {
             if (lane == 0) retire(s, item);
             __syncwarp();

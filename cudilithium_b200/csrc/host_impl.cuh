@@ -98,14 +98,14 @@ struct Impl {
 
     // One rejection round over nexec exec slots (exec LUT already on the device).
     static int sign_round(uint8_t *pool, size_t sp, size_t mlen, uint8_t *tpool, size_t tp, const uint32_t *d_exec,
-                          uint8_t *d_done, int nexec, cudaStream_t st) {
-        CUDIL_LAUNCH(KID_SIGN_EXPAND_MASK, st, k_sign_expand_mask<MODE><<<blocks_for((size_t)nexec * L), kBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec));
+                          uint8_t *d_done, int nexec, int nitems, cudaStream_t st) {
+        CUDIL_LAUNCH(KID_SIGN_EXPAND_MASK, st, k_sign_expand_mask<MODE><<<blocks_for((size_t)nexec * L), kBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec, nitems));
         CUDIL_CK_LAUNCH();
-        CUDIL_LAUNCH(KID_SIGN_COMPUTE_W, st, k_sign_compute_w<MODE, AW><<<(unsigned)((nexec + AW - 1) / AW), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, nexec));
+        CUDIL_LAUNCH(KID_SIGN_COMPUTE_W, st, k_sign_compute_w<MODE, AW><<<(unsigned)((nexec + AW - 1) / AW), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, nexec, nitems));
         CUDIL_CK_LAUNCH();
-        CUDIL_LAUNCH(KID_SIGN_CHALLENGE, st, k_sign_challenge<MODE><<<blocks_for((size_t)nexec, kItemBlock), kItemBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec));
+        CUDIL_LAUNCH(KID_SIGN_CHALLENGE, st, k_sign_challenge<MODE><<<blocks_for((size_t)nexec, kItemBlock), kItemBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec, nitems));
         CUDIL_CK_LAUNCH();
-        CUDIL_LAUNCH(KID_SIGN_REJECT, st, k_sign_reject<MODE><<<blocks_for((size_t)nexec * 16), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, d_done, nexec));
+        CUDIL_LAUNCH(KID_SIGN_REJECT, st, k_sign_reject<MODE><<<blocks_for((size_t)nexec * 16), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, d_done, nexec, nitems));
         CUDIL_CK_LAUNCH();
         return CUDIL_OK;
     }
@@ -156,7 +156,7 @@ struct Impl {
             }
             CUDIL_CK(cudaMemcpyAsync(lut->d_exec_lut, lut->h_exec_lut, sizeof(uint32_t) * T, cudaMemcpyHostToDevice, st));
             CUDIL_CK(cudaMemsetAsync(lut->d_done_lut, 0, T, st));
-            rc = sign_round(pool, sp, mlen, tpool, tp, lut->d_exec_lut, lut->d_done_lut, (int)T, st);
+            rc = sign_round(pool, sp, mlen, tpool, tp, lut->d_exec_lut, lut->d_done_lut, (int)T, (int)n, st);
             if (rc) return rc;
             CUDIL_CK(cudaMemcpyAsync(lut->h_done_lut, lut->d_done_lut, T, cudaMemcpyDeviceToHost, st));
             CUDIL_CK(cudaStreamSynchronize(st));
@@ -176,7 +176,7 @@ struct Impl {
                 CUDIL_CK(cudaMemcpyAsync(lut->d_copy_lut, lut->h_copy_lut, sizeof(cudil_copy_lut_element) * cc,
                                          cudaMemcpyHostToDevice, st));
                 CUDIL_LAUNCH(KID_SIG_COPY, st, k_sig_copy<MODE><<<(unsigned)cc, 128, 0, st>>>(pool, sp, tpool, tp,
-                                                               reinterpret_cast<const CopyEntry *>(lut->d_copy_lut)));
+                                                               reinterpret_cast<const CopyEntry *>(lut->d_copy_lut), T, n));
                 CUDIL_CK_LAUNCH();
             }
         }

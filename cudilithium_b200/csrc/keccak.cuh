@@ -251,6 +251,25 @@ __device__ __forceinline__ void shake_absorb_prefetch(uint32_t (&al)[25], uint32
     }
 }
 
+// Seeded randomized signing: rho' = SHAKE256(seed || le64(ctr), 64), 40 bytes in one SHAKE256 block
+// (seed as eight little-endian 32-bit words).
+__device__ __forceinline__ void derive_rhoprime(uint2 (&out)[8], const uint32_t (&seed)[8], unsigned long long ctr) {
+    uint32_t al[25], ah[25];
+    keccak_zero(al, ah);
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        al[w] = seed[2 * w];
+        ah[w] = seed[2 * w + 1];
+    }
+    al[4] = (uint32_t)ctr;
+    ah[4] = (uint32_t)(ctr >> 32);
+    al[5] = 0x1Fu;
+    ah[SHAKE256_RATE / 8 - 1] ^= 0x80000000u;
+    keccak_f1600(al, ah);
+#pragma unroll
+    for (int w = 0; w < 8; ++w) out[w] = make_uint2(al[w], ah[w]);
+}
+
 // Absorb of a short input of IN_LANES whole lanes plus an extra 16-bit little-endian nonce
 // (seed || nonce, as ExpandA/ExpandS/ExpandMask use); the input must fit one block.
 template <int RATE, int IN_LANES>

@@ -6,4 +6,7 @@
 namespace cudil {
 template struct Impl<2>;
 template struct EngineImpl<2>;
+
+// Error word of this translation unit's kernels in the bounds-checked build (see bounds.cuh).
+cudaError_t bounds_status_mode2(unsigned *out, bool reset) { return bounds_status_here(out, reset); }
 }  // namespace cudil

@@ -6,4 +6,7 @@
 namespace cudil {
 template struct Impl<5>;
 template struct EngineImpl<5>;
+
+// Error word of this translation unit's kernels in the bounds-checked build (see bounds.cuh).
+cudaError_t bounds_status_mode5(unsigned *out, bool reset) { return bounds_status_here(out, reset); }
 }  // namespace cudil

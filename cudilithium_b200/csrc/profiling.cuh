@@ -36,6 +36,7 @@ enum KernelId : int {
     KID_CACHE_PK,
     KID_SIG_CHECK,
     KID_SK_CHECK,
+    KID_DERIVE_RHOP,
     KID_COUNT
 };
 
@@ -45,7 +46,7 @@ inline const char *kernel_name(int id) {
         "k_sign_expand_mask", "k_sign_compute_w", "k_sign_challenge", "k_sign_reject", "k_sig_copy",
         "k_verify_prepare", "k_verify_w", "k_verify_final", "k_ntt_mul", "k_alu_peak",
         "k_fused_sign (graph)", "k_fused_verify (graph)", "k_fused_sched", "k_cache_sk", "k_cache_pk",
-        "k_sig_check", "k_sk_check"};
+        "k_sig_check", "k_sk_check", "k_derive_rhoprime"};
     return (id >= 0 && id < KID_COUNT) ? names[id] : "?";
 }
 

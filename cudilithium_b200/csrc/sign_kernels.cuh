@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_unpack_ntt(uint8_t *pool, size_
 // exec_lut entry = (item << 16) | nonce, as the reference's task_lut (src/api.cu:221-230).
 template <int MODE>
 __global__ void __launch_bounds__(kBlock) k_sign_expand_mask(const uint8_t *sign_pool, size_t sp, uint8_t *temp_pool,
-                                                             size_t tp, const uint32_t *exec_lut, int nexec) {
+                                                             size_t tp, const uint32_t *exec_lut, int nexec, int nitems) {
     using LY = Layout<MODE>;
     constexpr int L = Params<MODE>::L;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_expand_mask(const uint8_t *sign
     const int e = s / L, j = s % L;
     const uint32_t info = exec_lut[e];
     const uint32_t item = info >> 16, nonce = info & 0xFFFFu;
+    if (!bc_ok(item < (uint32_t)nitems, BC_STAGE_ITEM)) return;
     uint2 rhop[8];
     ld_lanes(rhop, sign_pool + (size_t)item * sp + LY::SG_RHOP);
     expand_mask_stream<MODE>(temp_pool + (size_t)e * tp + LY::TP_Y + (size_t)j * P<MODE>::POLYZ_PACKED, rhop,
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_expand_mask(const uint8_t *sign
 // computes w_i = invNTT(sum_j A_ij * y_hat_j), Decompose, w0 and packed w1.
 template <int MODE, int AW>
 __global__ void __launch_bounds__(kBlock) k_sign_compute_w(const uint8_t *sign_pool, size_t sp, size_t mlen, uint8_t *temp_pool,
-                                                           size_t tp, const uint32_t *exec_lut, int nexec) {
+                                                           size_t tp, const uint32_t *exec_lut, int nexec, int nitems) {
     using PM = P<MODE>;
     using LY = Layout<MODE>;
     constexpr int K = PM::K, L = PM::L;
@@ -175,6 +176,7 @@ __global__ void __launch_bounds__(kBlock) k_sign_compute_w(const uint8_t *sign_p
         const int a = u / K, i = u % K, e = e0 + a;
         if (e >= nexec) continue;
         const uint32_t item = exec_lut[e] >> 16;
+        if (!bc_ok(item < (uint32_t)nitems, BC_STAGE_ITEM)) continue;
         const int32_t *mat = reinterpret_cast<const int32_t *>(sign_pool + (size_t)item * sp + LY::sg_mat(mlen)) + (size_t)i * L * N;
         int32_t acc[16];
 #pragma unroll
@@ -269,7 +271,7 @@ __device__ __forceinline__ void sample_in_ball(const uint2 (&ct)[4], uint32_t *b
 // items still spread over every SM.
 template <int MODE, int TB = kItemBlock>
 __global__ void __launch_bounds__(TB) k_sign_challenge(const uint8_t *sign_pool, size_t sp, uint8_t *temp_pool, size_t tp,
-                                                       const uint32_t *exec_lut, int nexec) {
+                                                       const uint32_t *exec_lut, int nexec, int nitems) {
     using PM = P<MODE>;
     using LY = Layout<MODE>;
     __shared__ uint32_t s_blk[2 * 17][TB];
@@ -277,6 +279,7 @@ __global__ void __launch_bounds__(TB) k_sign_challenge(const uint8_t *sign_pool,
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nexec) return;
     const uint32_t item = exec_lut[e] >> 16;
+    if (!bc_ok(item < (uint32_t)nitems, BC_STAGE_ITEM)) return;
     uint8_t *trow = temp_pool + (size_t)e * tp;
     uint32_t al[25], ah[25];
     TwoPart src{sign_pool + (size_t)item * sp + LY::SG_MU, 8, trow + LY::TP_W1P, PM::W1PACKED_BYTES};
@@ -301,7 +304,8 @@ __global__ void __launch_bounds__(TB) k_sign_challenge(const uint8_t *sign_pool,
 // row holds the complete signature and done[e] = 1 (src/sign.cu:1010-1195).
 template <int MODE>
 __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_pool, size_t sp, size_t mlen, uint8_t *temp_pool,
-                                                        size_t tp, const uint32_t *exec_lut, uint8_t *done, int nexec) {
+                                                        size_t tp, const uint32_t *exec_lut, uint8_t *done, int nexec,
+                                                        int nitems) {
     using PM = P<MODE>;
     using LY = Layout<MODE>;
     constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA;
@@ -310,6 +314,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
     if (e >= nexec) return;
     Group g = make_group(sm, threadIdx.x >> 4);
     const uint32_t item = exec_lut[e] >> 16;
+    if (!bc_ok(item < (uint32_t)nitems, BC_STAGE_ITEM)) return;
     const uint8_t *srow = sign_pool + (size_t)item * sp;
     uint8_t *trow = temp_pool + (size_t)e * tp;
 
@@ -418,8 +423,10 @@ struct CopyEntry {
 };
 
 template <int MODE>
-__global__ void k_sig_copy(uint8_t *sign_pool, size_t sp, const uint8_t *temp_pool, size_t tp, const CopyEntry *lut) {
+__global__ void k_sig_copy(uint8_t *sign_pool, size_t sp, const uint8_t *temp_pool, size_t tp, const CopyEntry *lut,
+                           size_t nexec, size_t nitems) {
     const CopyEntry e = lut[blockIdx.x];
+    if (!bc_ok(e.exec_idx < nexec && e.sign_idx < nitems, BC_COPY_ENTRY)) return;
     const uint8_t *src = temp_pool + e.exec_idx * tp + Layout<MODE>::TP_SIG;
     uint8_t *dst = sign_pool + e.sign_idx * sp + Layout<MODE>::SG_SIG;
     for (int i = threadIdx.x; i < P<MODE>::SIG_BYTES; i += blockDim.x) dst[i] = src[i];

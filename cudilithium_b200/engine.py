@@ -114,12 +114,22 @@ class Engine:
         check(lib.cudil_engine_set_public_keys(self.h, d_pk.data_ptr(), n, _sp(stream)), "set_public_keys")
 
     def sign(self, d_sig: torch.Tensor, d_msgs: torch.Tensor, offsets, mlens, key_idx, stream=None,
-             d_rhoprime: torch.Tensor | None = None):
-        """d_rhoprime: optional device tensor of 64 random bytes per item (randomized signing)."""
+             d_rhoprime: torch.Tensor | None = None, rho_seed: bytes | None = None, rho_counter: int = 0):
+        """d_rhoprime: optional device tensor of 64 random bytes per item (randomized signing);
+        rho_seed: optional 32-byte seed from which the device derives every item's rho' as
+        SHAKE256(rho_seed || le64(rho_counter + i), 64) (seeded randomized signing)."""
         offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
         mlens = np.ascontiguousarray(mlens, dtype=np.uint32)
         key_idx = np.ascontiguousarray(key_idx, dtype=np.uint32)
         n = len(mlens)
+        if rho_seed is not None:
+            seed = bytes(rho_seed)
+            if len(seed) != 32:
+                raise ValueError("rho_seed must be 32 bytes")
+            check(lib.cudil_engine_sign_seeded(self.h, d_sig.data_ptr(), d_msgs.data_ptr(), d_msgs.numel(),
+                                               offsets.ctypes.data, mlens.ctypes.data, key_idx.ctypes.data, seed,
+                                               rho_counter, n, _sp(stream)), "cudil_engine_sign_seeded")
+            return
         if d_rhoprime is not None:
             check(lib.cudil_engine_sign_randomized(self.h, d_sig.data_ptr(), d_msgs.data_ptr(), d_msgs.numel(),
                                                    offsets.ctypes.data, mlens.ctypes.data, key_idx.ctypes.data,

@@ -109,6 +109,13 @@ int cudil_sign_randomized(int mode, uint8_t *sig, size_t sig_pitch, size_t *sigl
                           size_t mlen, const uint8_t *sk, const uint8_t *rhoprime, size_t rhoprime_pitch,
                           uint8_t *d_sign_pool, size_t sign_pool_pitch, uint8_t *d_temp_pool, size_t temp_pool_pitch,
                           cudil_task_lut *lut, size_t exec_threshold, size_t batch_size, void *stream);
+/* Device-side source of randomized-signing seeds (the reference draws rho' on the host with
+ * randombytes, src/api.cu:143-148): row i of d_rhoprime (rhoprime_pitch >= 64 bytes apart, device
+ * memory) = SHAKE256(seed || le64(counter + i), 64), a SHAKE256 XOF in counter mode keyed by one
+ * 32-byte seed from the caller's entropy source (host memory, read during the call).  Distinct
+ * (seed, counter) ranges give independent rho' values; reusing a range repeats them. */
+int cudil_derive_rhoprime(uint8_t *d_rhoprime, size_t rhoprime_pitch, const uint8_t *seed, unsigned long long counter,
+                          size_t n, void *stream);
 int cudil_sign_dev_randomized(int mode, uint8_t *d_sig, size_t sig_pitch, const uint8_t *d_m, size_t m_pitch,
                               size_t mlen, const uint8_t *d_sk, const uint8_t *d_rhoprime, size_t rhoprime_pitch,
                               uint8_t *d_sign_pool, size_t sign_pool_pitch, uint8_t *d_temp_pool,
@@ -236,6 +243,12 @@ int cudil_engine_sign(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, si
 int cudil_engine_sign_randomized(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
                                  const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx,
                                  const uint8_t *d_rhoprime, size_t n, void *stream);
+/* Seeded randomized signing through the engine: rho' of item i is derived on the device as
+ * SHAKE256(rho_seed || le64(rho_counter + i), 64) (cudil_derive_rhoprime's rule) inside the
+ * batch's prehash kernel; rho_seed is 32 bytes of host memory read during the call. */
+int cudil_engine_sign_seeded(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
+                             const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx,
+                             const uint8_t *rho_seed, unsigned long long rho_counter, size_t n, void *stream);
 int cudil_engine_verify(cudil_engine *e, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,
                         const unsigned long long *offsets, const uint32_t *mlens, const uint32_t *key_idx, size_t n,
                         void *stream);
@@ -350,6 +363,13 @@ int cudil_serve_trace(const cudil_serve_config *cfg, const uint8_t *const sk[3],
 /* Peak of the 32-bit LOP3/funnel-shift mix Keccak-f[1600] issues: launches `blocks` x 256 threads
  * doing `iters` x 32 ALU operations each; *ops_per_launch receives the operation count. */
 int cudil_alu_peak(uint32_t *d_out, int blocks, int iters, void *stream, double *ops_per_launch);
+
+/* Bounds-checked build (libcudilithium_b200_bc.so, built with `python cudilithium_b200/build.py
+ * --bounds-check`): device-side range checks of pool rows, attempt slots, item indices and key-cache
+ * rows record the first failing check's site code and skip the access instead of trapping.
+ * cudil_bounds_check_status stores that code in *error (0 = every check passed since the last
+ * reset) and clears it when reset != 0; in the normal library it returns CUDIL_ERR_INVALID. */
+int cudil_bounds_check_status(unsigned *error, int reset);
 
 /* Launch accounting.  cudil_launch_count: kernels launched by this library so far (process-wide).
  * cudil_kernel_timing(1) brackets every later launch with CUDA events on its stream (off by

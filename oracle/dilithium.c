@@ -385,6 +385,21 @@ void ora_seed_from_ctr(uint8_t seed[32], uint64_t ctr) {
     ora_shake128(seed, 32, b, 8);
 }
 
+/* Randomized-signing seeds derived from one 32-byte caller seed (the library's device-side hook for
+ * the reference's host randombytes(rhoprime) of src/api.cu:143-148): item i gets
+ * rho'_i = SHAKE256(seed || le64(counter + i), 64), an XOF in counter mode. */
+void ora_derive_rhoprime(uint8_t *out, const uint8_t seed[32], uint64_t counter, size_t n) {
+    uint8_t in[40];
+    size_t i;
+    int b;
+    memcpy(in, seed, 32);
+    for (i = 0; i < n; i++) {
+        const uint64_t c = counter + i;
+        for (b = 0; b < 8; b++) in[32 + b] = (uint8_t)(c >> (8 * b));
+        ora_shake256(out + 64 * i, 64, in, 40);
+    }
+}
+
 int ora_keypair_from_seed(int mode, uint8_t *pk, uint8_t *sk, const uint8_t seed[32]) {
     ora_params p;
     uint8_t seedbuf[128];

@@ -59,6 +59,7 @@ int ora_sign_rhoprime(int mode, uint8_t *sig, const uint8_t *m, size_t mlen, con
 int ora_verify(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen, const uint8_t *pk);
 int ora_sig_check(int mode, const uint8_t *sig);
 int ora_hint_check(int mode, const uint8_t *sig, int xor_lanes);
+void ora_derive_rhoprime(uint8_t *out, const uint8_t seed[32], uint64_t counter, size_t n);
 int ora_verify_xor_ballots(int mode, const uint8_t *sig, size_t siglen, const uint8_t *m, size_t mlen,
                            const uint8_t *pk);
 int ora_sk_check(int mode, const uint8_t *sk);

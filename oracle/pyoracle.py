@@ -54,6 +54,7 @@ def _load():
         "ora_sign_rhoprime": (c_int, [c_int, P8, P8, c_size_t, P8, P8, POINTER(c_int)]),
         "ora_sig_check": (c_int, [c_int, P8]),
         "ora_hint_check": (c_int, [c_int, P8, c_int]),
+        "ora_derive_rhoprime": (None, [P8, P8, c_uint64, c_size_t]),
         "ora_verify_xor_ballots": (c_int, [c_int, P8, c_size_t, P8, c_size_t, P8]),
         "ora_sk_check": (c_int, [c_int, P8]),
         "ora_verify": (c_int, [c_int, P8, c_size_t, P8, c_size_t, P8]),
@@ -161,6 +162,15 @@ def sign_rhoprime(mode: int, m: bytes, sk: np.ndarray, rhoprime: bytes) -> np.nd
     att = ctypes.c_int(0)
     assert lib.ora_sign_rhoprime(mode, _p(sig), _p(mb), len(m), _p(skb), _p(rp), ctypes.byref(att)) == 0
     return sig
+
+
+def derive_rhoprime(seed: bytes, counter: int, n: int) -> np.ndarray:
+    """(n, 64) randomized-signing seeds: rho'_i = SHAKE256(seed || le64(counter + i), 64)."""
+    out = np.zeros((max(n, 1), 64), np.uint8)
+    s = np.frombuffer(bytes(seed), np.uint8)
+    assert s.size == 32
+    lib.ora_derive_rhoprime(_p(out), _p(s), counter, n)
+    return out[:n]
 
 
 def sig_check(mode: int, sig: np.ndarray) -> np.ndarray:

@@ -146,3 +146,13 @@ def test_first_call_on_many_threads_is_deterministic():
             "assert np.array_equal(pk, pk1) and np.array_equal(sk, sk1)\n" % str(Path(__file__).resolve().parents[1]))
     for _ in range(3):
         subprocess.run([sys.executable, "-c", code], check=True)
+
+
+def test_derive_rhoprime_matches_shake256(oracle):
+    """The oracle's randomized-signing seed derivation against Python's own SHAKE256."""
+    seed = bytes(range(7, 39))
+    for counter in (0, 1, 2**32 - 1, 2**64 - 3):
+        got = oracle.derive_rhoprime(seed, counter, 3)
+        for i in range(3):
+            c = (counter + i) % 2**64
+            assert got[i].tobytes() == hashlib.shake_256(seed + c.to_bytes(8, "little")).digest(64)
