@@ -848,7 +848,8 @@ def run_serve(args, np) -> dict:
 
     for path, name in ((0, "fused"), (1, "plain")):
         cfgkw = dict(path=path, budget_bytes=budget, slots_per_lane=args.serve_slots, max_batch=args.serve_max_batch)
-        tr = tiled(max(len(base.reqs), int(args.serve_seconds * 4e6)), float("inf"))
+        # saturation: about one second of requests at the expected peak, all queued at t = 0
+        tr = tiled(max(len(base.reqs), int(min(args.serve_seconds, 1.0) * 4e6)), float("inf"))
         res, _, st = serve(tr, keys, want_sigs=False, **cfgkw)
         ok = bool(np.array_equal(res["status"][tr.reqs["op"] == 1], tr.expect[tr.reqs["op"] == 1]))
         sat = summary(tr, res, st)
@@ -1027,10 +1028,12 @@ def main():
                          "overlaps the next chunk's copy)")
     ap.add_argument("--serve-keys", type=int, default=4096, help="resident keys per parameter set (serving)")
     ap.add_argument("--serve-requests", type=int, default=200_000, help="distinct requests of the serving trace")
-    ap.add_argument("--serve-seconds", type=float, default=1.0, help="arrival window per serving point")
+    ap.add_argument("--serve-seconds", type=float, default=5.0, help="arrival window per serving point")
     ap.add_argument("--serve-fracs", type=float, nargs="+", default=[0.5, 0.8, 0.85, 0.9],
                     help="offered load as fractions of the saturation throughput")
-    ap.add_argument("--serve-slots", type=int, default=2, help="batch slots per (parameter set, op) lane")
+    ap.add_argument("--serve-slots", type=int, default=2,
+                    help="batch slots per (parameter set, op) lane; busier lanes get more in proportion to their "
+                         "share of the requests")
     ap.add_argument("--serve-max-batch", type=int, default=8192)
     ap.add_argument("--serve-budget-gib", type=float, default=48.0, help="device-memory budget of the server")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -65,7 +65,7 @@ class cudil_task_lut(ctypes.Structure):
 class cudil_serve_config(ctypes.Structure):
     _fields_ = [("device_budget_bytes", c_size_t), ("path", c_int32), ("slots_per_lane", c_int32),
                 ("max_batch", c_int32), ("engine_threads", c_int32), ("engine_spec_slots", c_int32),
-                ("plain_exec_threshold", c_int32), ("max_mlen", c_uint32), ("reserved", c_uint32)]
+                ("plain_exec_threshold", c_int32), ("max_mlen", c_uint32), ("lane_slots_by_load", c_uint32)]
 
 
 class cudil_serve_stats(ctypes.Structure):

@@ -403,8 +403,20 @@ extern "C" int cudil_serve_trace(const cudil_serve_config *cfg, const uint8_t *c
             for (size_t i = 0; i < nreq && !any; ++i) any = (mode_index(reqs[i].mode) == m && reqs[i].op == op);
             if (any) lanes.push_back(m * 2 + op);
         }
-    for (int k = 0; k < cfg->slots_per_lane && rc == CUDIL_OK; ++k) {
+    // slots per lane: slots_per_lane each, or (lane_slots_by_load) in proportion to the lane's share
+    // of the requests, never fewer than slots_per_lane
+    std::vector<int> want(6, cfg->slots_per_lane);
+    if (cfg->lane_slots_by_load && nreq) {
+        std::vector<size_t> count(6, 0);
+        for (size_t i = 0; i < nreq; ++i) ++count[mode_index(reqs[i].mode) * 2 + reqs[i].op];
+        const double total_slots = (double)cfg->slots_per_lane * (double)lanes.size();
+        for (int lane : lanes)
+            want[lane] = std::max(cfg->slots_per_lane, (int)(total_slots * (double)count[lane] / (double)nreq + 0.5));
+    }
+    const int max_want = *std::max_element(want.begin(), want.end());
+    for (int k = 0; k < max_want && rc == CUDIL_OK; ++k) {
         for (int lane : lanes) {
+            if (k >= want[lane]) continue;
             const int m = lane / 2, op = lane % 2;
             size_t remaining = 0;
             if (cfg->device_budget_bytes) {

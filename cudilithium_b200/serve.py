@@ -139,9 +139,11 @@ def sign_messages(mode: int, keys: Keys, msgs: list, key_idx: np.ndarray) -> np.
 
 
 def serve(tr: Trace, keys: Keys, path: int = 0, budget_bytes: int = 0, slots_per_lane: int = 2, max_batch: int = 8192,
-          threads: int = 0, spec_slots: int = 0, plain_exec_threshold: int = 0, want_sigs: bool = True):
-    """Replays `tr` through cudil_serve_trace.  Returns (results[RESULT_DTYPE], signatures
-    (n, max sig bytes) or None, stats dict)."""
+          threads: int = 0, spec_slots: int = 0, plain_exec_threshold: int = 0, want_sigs: bool = True,
+          slots_by_load: bool = True):
+    """Replays `tr` through cudil_serve_trace.  slots_by_load: lanes get batch slots in proportion
+    to their share of the requests (at least slots_per_lane).  Returns (results[RESULT_DTYPE],
+    signatures (n, max sig bytes) or None, stats dict)."""
     from .autotune import tuned
     n = len(tr.reqs)
     cfg = _lib.cudil_serve_config()
@@ -154,6 +156,7 @@ def serve(tr: Trace, keys: Keys, path: int = 0, budget_bytes: int = 0, slots_per
     cfg.engine_spec_slots = spec_slots or t["spec_slots"]
     cfg.plain_exec_threshold = plain_exec_threshold or max(1024, max_batch)
     cfg.max_mlen = max(1, int(tr.reqs["mlen"].max()) if n else 1)
+    cfg.lane_slots_by_load = 1 if slots_by_load else 0
     sk = (ctypes.c_void_p * 3)()
     pk = (ctypes.c_void_p * 3)()
     nk = (ctypes.c_size_t * 3)()

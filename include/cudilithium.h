@@ -306,7 +306,8 @@ int cudil_engine_info(const cudil_engine *e, int *mode, int *threads, int *sign_
  *
  * cudil_serve_trace replays an open-loop trace in real time on the current device.  Request i
  * becomes visible arrival_s seconds after the start and queues in the FIFO of its (parameter set,
- * operation) lane.  Each lane owns up to slots_per_lane batch slots (stream + device buffers); a
+ * operation) lane.  Each lane owns up to slots_per_lane batch slots (stream + device buffers, more
+ * for busy lanes with lane_slots_by_load); a
  * free slot takes everything queued in its lane (at most max_batch) as one batch, so batches of
  * every lane overlap on the device while new requests queue.  Slots are created only while the
  * device-memory estimate stays within device_budget_bytes (0 = unlimited); every lane in use
@@ -342,7 +343,10 @@ typedef struct {
     int32_t engine_spec_slots;    /* fused: signer speculation target (0 = default) */
     int32_t plain_exec_threshold; /* plain: signing attempts per round (>= 1) */
     uint32_t max_mlen;
-    uint32_t reserved;
+    /* 0: every lane gets slots_per_lane slots; 1: a lane gets slots in proportion to its share of
+     * the trace's requests, round(share * slots_per_lane * lanes), at least slots_per_lane (a lane
+     * that carries most of the requests also needs more host threads staging its batches) */
+    uint32_t lane_slots_by_load;
 } cudil_serve_config;
 
 typedef struct {
