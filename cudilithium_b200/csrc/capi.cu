@@ -76,18 +76,22 @@ __global__ void __launch_bounds__(kBlock) k_ntt_mul(const int32_t *a, const int3
     long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
     if (p >= npolys) return;
     Group g = make_group(sm, threadIdx.x >> 4);
+    // the thread's twiddles depend only on its group position: loaded once for every polynomial
+    int2 twf[16], twi[16];
+    load_tw16(twf, g_group_tw.fwd[g.t]);
+    load_tw16(twi, g_group_tw.inv[g.t]);
     int32_t x[16], y[16];
     load16_strided(x, a + p * N, g.t);
 #pragma unroll 1
     for (; p < npolys; p += groups) {
         load16_contig(y, b + p * N + 16 * g.t);
-        ntt16(x, g.sm, g.gmask, g.t);
+        ntt16_tw<false>(x, g.sm, g.gmask, g.t, twf);
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = montmul(x[m], y[m]);
         const long long nx = p + groups;
         int32_t xn[16];
         if (nx < npolys) load16_strided(xn, a + nx * N, g.t);
-        intt16(x, g.sm, g.gmask, g.t);
+        intt16_tw<false>(x, g.sm, g.gmask, g.t, twi);
         store16_strided(out + p * N, x, g.t);
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = xn[m];

@@ -74,9 +74,17 @@ __device__ __forceinline__ int32_t bfly_mul(int32_t b, int32_t z, int32_t zq) {
 
 template <bool S = false>
 __device__ __forceinline__ void ct_bfly(int32_t &a, int32_t &b, int32_t z, int32_t zq) {
-    int32_t t = bfly_mul<S>(b, z, zq);
-    b = a - t;
-    a = a + t;
+    if constexpr (S) {
+        int32_t t = bfly_mul<S>(b, z, zq);
+        b = a - t;
+        a = a + t;
+    } else {
+        // montmul_pre(b, z, zq) = hi(b z) - hi((b zq) q): the two outputs as three-input adds
+        // a +/- hi(b z) -/+ hi((b zq) q), with no separate difference (same values)
+        const int32_t h1 = __mulhi(b, z), h2 = __mulhi(b * zq, Q);
+        b = a - h1 + h2;
+        a = a + h1 - h2;
+    }
 }
 
 template <bool S = false>
@@ -101,9 +109,10 @@ __device__ __forceinline__ void load_tw16(int2 (&tw)[16], const int2 *src) {
     }
 }
 
-// Forward NTT; sm = this group's NTT_SMEM_WORDS-word region, gmask = this group's lanes.
+// Forward NTT with the thread's register-local twiddles already loaded (tw = the group position's
+// row of GroupTwiddles::fwd); sm = this group's NTT_SMEM_WORDS-word region, gmask = its lanes.
 template <bool S>
-__device__ __forceinline__ void ntt16_t(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
+__device__ __forceinline__ void ntt16_tw(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t, const int2 (&tw)[16]) {
     // len 128: (i, i+8), zeta[1]
 #pragma unroll
     for (int i = 0; i < 8; ++i) ct_bfly<S>(x[i], x[i + 8], utw<S>().zeta[1], utw<S>().zeta_q[1]);
@@ -127,8 +136,6 @@ __device__ __forceinline__ void ntt16_t(int32_t (&x)[16], int32_t *sm, unsigned 
     for (int i = 0; i < 16; ++i) x[i] = sm[17 * t + i];
     __syncwarp(gmask);
 
-    int2 tw[16];
-    load_tw16(tw, (S ? g_group_tw_s : g_group_tw).fwd[t]);
     // len 8: (i, i+8), zeta[16+t]
 #pragma unroll
     for (int i = 0; i < 8; ++i) ct_bfly<S>(x[i], x[i + 8], tw[0].x, tw[0].y);
@@ -145,11 +152,18 @@ __device__ __forceinline__ void ntt16_t(int32_t (&x)[16], int32_t *sm, unsigned 
     for (int i = 0; i < 16; i += 2) ct_bfly<S>(x[i], x[i + 1], tw[7 + (i >> 1)].x, tw[7 + (i >> 1)].y);
 }
 
-// Inverse NTT including the final multiplication by f (invntt_tomont).
+// Forward NTT; sm = this group's NTT_SMEM_WORDS-word region, gmask = this group's lanes.
 template <bool S>
-__device__ __forceinline__ void intt16_t(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
+__device__ __forceinline__ void ntt16_t(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
     int2 tw[16];
-    load_tw16(tw, (S ? g_group_tw_s : g_group_tw).inv[t]);
+    load_tw16(tw, (S ? g_group_tw_s : g_group_tw).fwd[t]);
+    ntt16_tw<S>(x, sm, gmask, t, tw);
+}
+
+// Inverse NTT including the final multiplication by f (invntt_tomont), register-local twiddles
+// already loaded (tw = the group position's row of GroupTwiddles::inv).
+template <bool S>
+__device__ __forceinline__ void intt16_tw(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t, const int2 (&tw)[16]) {
     // len 1: block 8t + (i>>1): -zeta[255 - 8t - (i>>1)]
 #pragma unroll
     for (int i = 0; i < 16; i += 2) gs_bfly<S>(x[i], x[i + 1], tw[i >> 1].x, tw[i >> 1].y);
@@ -188,6 +202,13 @@ __device__ __forceinline__ void intt16_t(int32_t (&x)[16], int32_t *sm, unsigned
     for (int i = 0; i < 8; ++i) gs_bfly<S>(x[i], x[i + 8], utw<S>().izeta[1], utw<S>().izeta_q[1]);
 #pragma unroll
     for (int i = 0; i < 16; ++i) x[i] = montmul_pre(x[i], F_INV, F_INV_Q);
+}
+
+template <bool S>
+__device__ __forceinline__ void intt16_t(int32_t (&x)[16], int32_t *sm, unsigned gmask, int t) {
+    int2 tw[16];
+    load_tw16(tw, (S ? g_group_tw_s : g_group_tw).inv[t]);
+    intt16_tw<S>(x, sm, gmask, t, tw);
 }
 
 // Montgomery transforms: the reference's exact output representatives (key generation, the NTT
