@@ -1,7 +1,7 @@
 // Host side of the fused engine: device buffers sized once at creation, per-key caches, and the
 // graph that runs a whole signing (or verification) batch on the device with one launch:
 //   [k_fused_init] -> [k_fused_prehash] -> [k_fused_sign]       (sign)
-//   [k_fused_init] -> [k_fused_verify]                           (verify)
+//   [k_fused_init] -> [k_fused_verify_prehash] -> [k_fused_verify] (verify)
 // The batch size travels in device memory (FusedQueue::n), so one instantiated graph serves every
 // batch size up to the engine's capacity; only the per-item metadata upload precedes the launch.
 #pragma once
@@ -367,9 +367,10 @@ struct EngineImpl : EngineBase {
     template <int T>
     void record_verify(cudaStream_t st, int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs) {
         MsgRefs mr{d_msgs, d_off, d_mlen, d_key, d_order, nullptr, (unsigned)max_keys};
-        k_fused_init<<<1, 32, 0, st>>>(q, best, locks, nullptr, nullptr);
+        k_fused_init<<<1, 32, 0, st>>>(q, nullptr, nullptr, nullptr, nullptr);
+        k_fused_verify_prehash<MODE><<<prehash_grid, kPrehashBlock, 0, st>>>(pk_cache, pk_pitch, mr, items, q);
         k_fused_verify<MODE, T><<<verify_grid, T, verify_smem, st>>>(pk_cache, pk_pitch, mr, d_sig, PM::SIG_BYTES, d_ret,
-                                                                    scratch, q);
+                                                                    scratch, items, q);
         cudaMemcpyAsync(h_status, q, sizeof(FusedQueue), cudaMemcpyDeviceToHost, st);
     }
 
@@ -480,7 +481,7 @@ struct EngineImpl : EngineBase {
             d_msgs = reinterpret_cast<const uint8_t *>(items);
         }
         if (((uintptr_t)d_msgs) & 7u) return CUDIL_ERR_INVALID;
-        int rc = upload_meta(off, mlen, key, n, n_pk, msgs_bytes, false, st);
+        int rc = upload_meta(off, mlen, key, n, n_pk, msgs_bytes, true, st);
         if (rc) return rc;
         if (!g_verify || g_verify_key[0] != d_ret || g_verify_key[1] != d_sig || d_msgs != g_verify_msgs) {
             rc = capture(st, &g_verify, false, reinterpret_cast<uint8_t *>(d_ret), d_sig, d_msgs);

@@ -249,11 +249,12 @@ __global__ void __launch_bounds__(kPrehashBlock) k_fused_prehash(const uint8_t *
     }
 }
 
-// Resets the per-item winner state and the queue for q->n items (n set by the host copy).
+// Resets the queue and, for signing, the per-item winner state of q->n items (n set by the host
+// copy; best == nullptr: queue only).
 static __global__ void k_fused_init(FusedQueue *q, unsigned *best, unsigned *locks, unsigned *next_nonce,
                                     unsigned *inflight) {
     const unsigned n = q->n;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; best && i < n; i += gridDim.x * blockDim.x) {
         best[i] = 0xFFFFFFFFu;
         locks[i] = 0u;
         if (next_nonce) next_nonce[i] = 0u;
@@ -822,6 +823,29 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
 
 // ------------------------------------------------------------------ persistent verifier
 
+// mu = H(tr || m) of every signature of a verification batch, ahead of the persistent verifier
+// (as k_fused_prehash for signing): one thread per message, longest first, one warp per block, the
+// absorb with the next block's lanes in flight.  A long message therefore costs its own
+// permutations on one thread instead of stalling a verifier block's first phase.
+template <int MODE>
+__global__ void __launch_bounds__(kPrehashBlock) k_fused_verify_prehash(const uint8_t *cache, size_t cpitch, MsgRefs mr,
+                                                                        uint8_t *items, const FusedQueue *q) {
+    using C = Cache<MODE>;
+    const unsigned n = q->n;
+    for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const unsigned it = mr.order[r];
+        if (!bc_ok(it < n && mr.key_idx[it] < mr.nkeys, BC_PREHASH_ITEM)) continue;
+        const uint8_t *row = cache + (size_t)mr.key_idx[it] * cpitch;
+        uint32_t al[25], ah[25];
+        TwoPart src{row + C::PK_TR, 4, mr.msgs + mr.offsets[it], (long long)mr.mlens[it]};
+        shake_absorb_prefetch<SHAKE256_RATE>(al, ah, src, (long long)SEEDBYTES + mr.mlens[it]);
+        keccak_f1600(al, ah);
+        uint2 *out = reinterpret_cast<uint2 *>(items + (size_t)it * C::ITEM_BYTES);
+#pragma unroll
+        for (int w = 0; w < 8; ++w) out[w] = make_uint2(al[w], ah[w]);
+    }
+}
+
 template <int MODE, int THREADS>
 struct FusedVerifySmem {
     using PM = P<MODE>;
@@ -834,7 +858,7 @@ struct FusedVerifySmem {
 template <int MODE, int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const uint8_t *cache, size_t cpitch, MsgRefs mr,
                                                           const uint8_t *sig, size_t sig_pitch, int *ret,
-                                                          uint8_t *scratch, FusedQueue *q) {
+                                                          uint8_t *scratch, const uint8_t *items, FusedQueue *q) {
     using PM = P<MODE>;
     using C = Cache<MODE>;
     constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA, A = THREADS, G = THREADS / 16;
@@ -854,15 +878,12 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
         if (base >= n) break;
         const int na = (int)((n - base) < chunk ? (n - base) : chunk);
 
-        // hint encoding checks, mu = H(tr||m), c = SampleInBall(c~): thread per signature
+        // hint encoding checks, mu (from the prehash kernel), c = SampleInBall(c~): thread per signature
         if (tid < na) {
             const unsigned it = base + tid;
             const uint8_t *s = sig + (size_t)it * sig_pitch;
-            const unsigned key = mr.key_idx[it];
-            const bool key_ok = bc_ok(key < mr.nkeys, BC_VERIFY_KEY);
-            const uint8_t *row = cache + (size_t)(key_ok ? key : 0u) * cpitch;
             uint8_t *slot = my_slots + (size_t)tid * C::VSLOT;
-            int status = key_ok ? 0 : 4;
+            int status = bc_ok(mr.key_idx[it] < mr.nkeys, BC_VERIFY_KEY) ? 0 : 4;
             const uint8_t *h = s + PM::SIG_H;
             int k = 0;
             for (int i = 0; i < K && !status; ++i) {
@@ -878,13 +899,11 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
             if (!status)
                 for (int j = k; j < OMEGA; ++j)
                     if (h[j]) status = 1;
-            uint32_t al[25], ah[25];
-            TwoPart src{row + C::PK_TR, 4, mr.msgs + mr.offsets[it], (long long)mr.mlens[it]};
-            shake_absorb<SHAKE256_RATE>(al, ah, src, (long long)SEEDBYTES + mr.mlens[it]);
-            keccak_f1600(al, ah);
+            uint2 mu8[8];
+            ld_lanes(mu8, items + (size_t)it * C::ITEM_BYTES);
             uint2 *mu = reinterpret_cast<uint2 *>(slot + C::VS_MU);
 #pragma unroll
-            for (int w = 0; w < 8; ++w) mu[w] = make_uint2(al[w], ah[w]);
+            for (int w = 0; w < 8; ++w) mu[w] = mu8[w];
             uint2 ct[4];
 #pragma unroll
             for (int w = 0; w < 4; ++w) ct[w] = make_uint2(load_lane_bytes(s + 8 * w, 8).x, load_lane_bytes(s + 8 * w, 8).y);
