@@ -320,15 +320,17 @@ struct EngineImpl : EngineBase {
         unsigned *hm = hk + max_items;
         unsigned *ho = hm + max_items;
         unsigned long long *hoff = reinterpret_cast<unsigned long long *>(ho + max_items);
+        bool descending = true;  // already longest first (every batch of equal lengths is)
         for (size_t i = 0; i < n; ++i) {
             if (key[i] >= nkeys || (off[i] & 7u) || off[i] > msgs_bytes || mlen[i] > msgs_bytes - off[i])
                 return CUDIL_ERR_INVALID;
             hk[i] = key[i];
             hm[i] = mlen[i];
             hoff[i] = off[i];
+            if (i && mlen[i] > mlen[i - 1]) descending = false;
         }
         std::iota(ho, ho + n, 0u);
-        if (longest_first)
+        if (longest_first && !descending)
             std::stable_sort(ho, ho + n, [&](unsigned a, unsigned b) { return hm[a] > hm[b]; });
         CUDIL_CK(cudaMemcpyAsync(q, hq, sizeof(FusedQueue), cudaMemcpyHostToDevice, st));
         CUDIL_CK(cudaMemcpyAsync(d_key, hk, n * sizeof(unsigned), cudaMemcpyHostToDevice, st));
