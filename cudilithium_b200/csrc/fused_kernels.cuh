@@ -467,7 +467,10 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
     auto keccak_phase = [&](int cb, int na_c, int nb, int na_n) {
         uint32_t *blkw = reinterpret_cast<uint32_t *>(ph) + tid;
         uint32_t *mask = reinterpret_cast<uint32_t *>(ph) + 34 * THREADS + tid;
-        const int total = na_c + na_n * L;
+        // ExpandMask jobs start at a multiple of 32, so no warp holds both job types (a warp runs
+        // divergent branches one after the other: a mixed warp would take 8 + 5 permutations)
+        const int cpad = (na_c + 31) & ~31;
+        const int total = cpad + na_n * L;
         // a warp takes 32 consecutive jobs at a time, so its lanes run the same job type together
 #pragma unroll 1
         for (;;) {
@@ -498,8 +501,8 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                         mo[k] = make_uint4(mask[(4 * k) * THREADS], mask[(4 * k + 1) * THREADS], mask[(4 * k + 2) * THREADS],
                                            mask[(4 * k + 3) * THREADS]);
                 }
-            } else if (job < total) {
-                const int idx = job - na_c, a = idx / L, j = idx % L;
+            } else if (job >= cpad && job < total) {
+                const int idx = job - cpad, a = idx / L, j = idx % L;
                 const bool slot_ok = bc_ok(a < A, BC_SIGN_SLOT);
                 const unsigned item = slot_ok ? s_item[nb * A + a] : 0xFFFFFFFFu, nonce = slot_ok ? s_nonce[nb * A + a] : 0u;
                 if (bc_ok(item < n, BC_SIGN_SLOT) && !(__ldcg(arg.best + item) < nonce)) {
@@ -761,7 +764,10 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
 
     // ---------------- NTT phase: rejection of batch cb (jobs < na_c), w = A y of batch nb
     auto ntt_phase = [&](int cb, int na_c, int nb, int na_n) {
-        const int total = na_c + na_n;
+        // w jobs start at an even index, so the two groups of a warp never run a rejection and a w
+        // job side by side (divergent: the warp would run one after the other)
+        const int rpad = (na_c + 1) & ~1;
+        const int total = rpad + na_n;
         // a warp takes two consecutive jobs, one per 16-thread group, so both groups of the warp
         // usually run the same job type in lockstep
 #pragma unroll 1
@@ -771,12 +777,10 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
             base = __shfl_sync(0xFFFFFFFFu, base, 0);
             if ((int)base >= total) break;
             const int job = (int)base + (lane_off ? 1 : 0);
-            if (job < total) {
-                if (job < na_c)
-                    reject_job(cb, job);
-                else
-                    w_job(nb, job - na_c);
-            }
+            if (job < na_c)
+                reject_job(cb, job);
+            else if (job >= rpad && job < total)
+                w_job(nb, job - rpad);
             __syncwarp();  // both groups back together before the next full-warp grab
         }
     };
