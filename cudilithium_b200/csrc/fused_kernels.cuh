@@ -516,18 +516,21 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         }
     };
 
-    // rejection checks, hints and publication of one attempt (group-collective)
+    // rejection checks, hints and publication of one attempt (warp-collective).  The two groups
+    // of the warp take the attempt's polynomials in pairs (poly 2p + half), so they follow the same
+    // control flow: a rejection ends the job for the whole warp, and no group waits for another
+    // group's longer attempt.
     auto reject_job = [&](int cb, int a) {
-        // (range checks of the bounds-checked build: every value is the same across the group)
+        // (range checks of the bounds-checked build: every value is the same across the warp)
         if (!bc_ok(a < A, BC_SIGN_SLOT)) return;
         const unsigned item = s_item[cb * A + a], nonce = s_nonce[cb * A + a];
         if (!bc_ok(item < n, BC_SIGN_SLOT)) return;
-        // one decision per group: out-of-range nonce, or a smaller nonce of the item already accepted
+        // one decision per warp: out-of-range nonce, or a smaller nonce of the item already accepted
         bool skip = nonce > 0xFFFFu || __ldcg(arg.best + item) < nonce;
-        skip = __shfl_sync(g.gmask, skip, lane_off);
+        skip = __shfl_sync(0xFFFFFFFFu, skip, 0);
         const unsigned key = arg.key_idx[item];
         if (skip || !bc_ok(key < arg.nkeys, BC_SIGN_KEY)) {
-            if (g.t == 0) atomicSub(arg.inflight + item, 1u);
+            if (lane == 0) atomicSub(arg.inflight + item, 1u);
             return;
         }
         uint8_t *slot = slot_of(cb, a);
@@ -545,6 +548,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                 masks[4 * k + 3] = v.w;
             }
         }
+        // both groups transform c (same data, same instructions)
         int32_t ch[16];
         challenge_strided(ch, masks, g.t);
         fwd(ch);
@@ -552,125 +556,146 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         const int32_t *s2 = reinterpret_cast<const int32_t *>(row + C::SK_S2);
         const int32_t *t0 = reinterpret_cast<const int32_t *>(row + C::SK_T0);
         uint8_t *hs = slot + C::SL_SIG + PM::SIG_H;
+        const int half = lane_off >> 4;
         bool rejected = false;
-        int cnt = 0, n_intt = 0;
-        int32_t nx[16];
-        // Acceptance needs every check to pass, so the checks run most selective first: steps
-        // r0_0..r0_{K-1} (r0 replaces w0 in the slot, for the hints), z_0..z_{L-1}, then
-        // ct0_0..ct0_{K-1} with the hints.  While one step transforms, the next step's key
-        // operand and (inlined transforms) this step's slot data (y_j, or w0_i / r0_i) are in
-        // flight.
+        int n_intt = 0, cnt = 0;
+        // Acceptance needs every check to pass, so the checks run most selective first: pair steps
+        // of the r0_i (r0 replaces w0 in the slot, for the hints), then of the z_j, then of the
+        // ct0_i with the hints.  K is even for every parameter set; L is odd for two of them, so
+        // the last z pair may leave the second group without a polynomial (it transforms zeros
+        // and stores nothing).  While one step transforms, the next step's key rows and (inlined
+        // transforms) this step's slot data are in flight.
+        constexpr int PR = K / 2, PZ = (L + 1) / 2, NSTEP = 2 * PR + PZ;
         auto operand = [&](int step) -> const int32_t * {
-            if (step < K) return s2 + (size_t)step * N;
-            if (step < K + L) return s1 + (size_t)(step - K) * N;
-            return t0 + (size_t)(step - K - L) * N;
+            if (step < PR) return s2 + (size_t)(2 * step + half) * N;
+            if (step < PR + PZ) {
+                const int j = 2 * (step - PR) + half;
+                return s1 + (size_t)(j < L ? j : L - 1) * N;
+            }
+            return t0 + (size_t)(2 * (step - PR - PZ) + half) * N;
         };
+        int32_t nx[16];
         load16_contig(nx, operand(0) + 16 * g.t);
 #pragma unroll 1
-        for (int step = 0; step < L + 2 * K; ++step) {
-            const bool is_r0 = step < K, is_z = !is_r0 && step < K + L;
-            const int i = is_r0 ? step : step - K - L;
+        for (int step = 0; step < NSTEP; ++step) {
+            const bool is_r0 = step < PR, is_z = !is_r0 && step < PR + PZ;
+            const int k = 2 * (is_r0 ? step : (is_z ? step - PR : step - PR - PZ)) + half;  // i, or j for z
+            const bool act = !is_z || k < L;
             int32_t x[16];
 #pragma unroll
-            for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], nx[m]);
-            if (step + 1 < L + 2 * K) load16_contig(nx, operand(step + 1) + 16 * g.t);
-            // slot data of this step (y_j, or w0_i / r0_i); with the out-of-line transform a load in
-            // flight across the call would be spilled, so there it is read after the transform
-            const int32_t *w0c = reinterpret_cast<const int32_t *>(slot + C::SL_W0) + (size_t)i * N;
+            for (int m = 0; m < 16; ++m) x[m] = act ? montmul(ch[m], nx[m]) : 0;
+            if (step + 1 < NSTEP) load16_contig(nx, operand(step + 1) + 16 * g.t);
+            int32_t *w0 = reinterpret_cast<int32_t *>(slot + C::SL_W0) + (size_t)(is_z ? 0 : k) * N;
+            const uint8_t *yp = slot + C::SL_Y + (size_t)(act ? k : 0) * PM::POLYZ_PACKED;
             int32_t pre[16];
-            if constexpr (MODE == 2) {
+            // the slot data of the step: with the inlined transform it is in flight across it; the
+            // out-of-line transform would spill a load held across the call, so there it is read
+            // afterwards
+            auto load_pre = [&] {
                 if (is_z) {
-                    unpack_z_strided<MODE>(pre, slot + C::SL_Y + (size_t)(step - K) * PM::POLYZ_PACKED, g.t);
-                } else {
+                    unpack_z_strided<MODE>(pre, yp, g.t);
 #pragma unroll
-                    for (int m = 0; m < 16; ++m) pre[m] = w0c[g.t + 16 * m];
+                    for (int m = 0; m < 16; ++m) pre[m] = act ? pre[m] : 0;
+                } else {
+                    load16_strided(pre, w0, g.t);
                 }
-            }
+            };
+            if constexpr (MODE == 2) load_pre();
             inv(x);
-            ++n_intt;
+            n_intt += act ? 1 : 0;
+            if constexpr (MODE != 2) load_pre();
             bool bad = false;
             if (is_z) {
-                const int j = step - K;
-                if constexpr (MODE != 2) unpack_z_strided<MODE>(pre, slot + C::SL_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
                     x[m] = reduce32(x[m] + pre[m]);
-                    bad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
+                    bad |= act && exceeds(x[m], PM::GAMMA1 - PM::BETA);
                 }
-                if (group_any(g, bad)) {
+                if (__ballot_sync(0xFFFFFFFFu, bad)) {
                     rejected = true;
                     break;
                 }
                 int32_t zc[16];
                 strided_to_contig(g, x, zc);
-                uint32_t v[16];
+                if (act) {
+                    uint32_t v[16];
 #pragma unroll
-                for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
-                pack16_words<PM::Z_BITS>(
-                    reinterpret_cast<uint32_t *>(slot + C::SL_SIG + PM::SIG_Z + (size_t)j * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
+                    for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
+                    pack16_words<PM::Z_BITS>(
+                        reinterpret_cast<uint32_t *>(slot + C::SL_SIG + PM::SIG_Z + (size_t)k * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
+                }
             } else if (is_r0) {
-                int32_t *w0 = reinterpret_cast<int32_t *>(slot + C::SL_W0) + (size_t)i * N;
-                int32_t r0[16];
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
-                    r0[m] = reduce32((MODE == 2 ? pre[m] : w0c[g.t + 16 * m]) - x[m]);
-                    bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
+                    pre[m] = reduce32(pre[m] - x[m]);
+                    bad |= exceeds(pre[m], PM::GAMMA2 - PM::BETA);
                 }
-                if (group_any(g, bad)) {
+                if (__ballot_sync(0xFFFFFFFFu, bad)) {
                     rejected = true;
                     break;
                 }
-#pragma unroll
-                for (int m = 0; m < 16; ++m) w0[g.t + 16 * m] = r0[m];
+                store16_strided(w0, pre, g.t);
             } else {
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
                     x[m] = reduce32(x[m]);
                     bad |= exceeds(x[m], PM::GAMMA2);
                 }
-                if (group_any(g, bad)) {
+                if (__ballot_sync(0xFFFFFFFFu, bad)) {
                     rejected = true;
                     break;
                 }
-                const uint8_t *w1p = slot + C::SL_W1P + (size_t)i * PM::POLYW1_PACKED;
+                // hint bits of poly k: bit m of hb = hint of coefficient t + 16 m
+                const uint8_t *w1p = slot + C::SL_W1P + (size_t)k * PM::POLYW1_PACKED;
+                unsigned hb = 0;
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
                     const int32_t w1 = (int32_t)get_bits(w1p, (g.t + 16 * m) * PM::W1_BITS, PM::W1_BITS);
-                    const unsigned h = make_hint<MODE>((MODE == 2 ? pre[m] : w0c[g.t + 16 * m]) + x[m], w1);
-                    const unsigned bal = (__ballot_sync(g.gmask, h) >> lane_off) & 0xFFFFu;
-                    if (h) {
-                        const int idx = cnt + __popc(bal & ((1u << g.t) - 1u));
-                        if (idx < OMEGA) hs[idx] = (uint8_t)(g.t + 16 * m);
-                    }
-                    cnt += __popc(bal);
+                    hb |= make_hint<MODE>(pre[m] + x[m], w1) << m;
                 }
-                if (cnt > OMEGA) {
+                // hint counts of both polynomials of the pair (sums over each group), then the
+                // positions in ascending coefficient order: poly 2p first, then poly 2p + 1
+                int tot = __popc(hb);
+#pragma unroll
+                for (int o = 8; o >= 1; o >>= 1) tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+                const int tot0 = __shfl_sync(0xFFFFFFFFu, tot, 0), tot1 = __shfl_sync(0xFFFFFFFFu, tot, 16);
+                if (cnt + tot0 + tot1 > OMEGA) {
                     rejected = true;
                     break;
                 }
-                if (g.t == 0) hs[OMEGA + i] = (uint8_t)cnt;
+                int idx = cnt + (half ? tot0 : 0);
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const unsigned bit = (hb >> m) & 1u;
+                    const unsigned bal = (__ballot_sync(0xFFFFFFFFu, bit) >> lane_off) & 0xFFFFu;
+                    if (bit) hs[idx + __popc(bal & ((1u << g.t) - 1u))] = (uint8_t)(g.t + 16 * m);
+                    idx += __popc(bal);
+                }
+                if (g.t == 0) hs[OMEGA + k] = (uint8_t)(cnt + (half ? tot0 + tot1 : tot0));
+                cnt += tot0 + tot1;
             }
         }
-        if (g.t == 0) {
+        n_intt += __shfl_down_sync(0xFFFFFFFFu, n_intt, 16);  // lane 0: both groups
+        if (lane == 0) {
             atomicAdd(&q->intt, (unsigned long long)n_intt);
             atomicSub(arg.inflight + item, 1u);
         }
         if (rejected) return;
-        for (int qq = cnt + g.t; qq < OMEGA; qq += 16) hs[qq] = 0;
-        __syncwarp(g.gmask);
+        for (int qq = cnt + lane; qq < OMEGA; qq += 32) hs[qq] = 0;
+        __syncwarp();
         // accepted: lower the item's best nonce; publish if this attempt holds the minimum
         unsigned old = 0;
-        if (g.t == 0) old = atomicMin(arg.best + item, nonce);
-        old = __shfl_sync(g.gmask, old, lane_off);
+        if (lane == 0) old = atomicMin(arg.best + item, nonce);
+        old = __shfl_sync(0xFFFFFFFFu, old, 0);
         if (nonce >= old) return;
-        if (g.t == 0 && old == 0xFFFFFFFFu) {
+        if (lane == 0 && old == 0xFFFFFFFFu) {
             atomicAdd(&q->done_items, 1u);
             atomicSub(&s_ctl[CT_PEND], 1u);
         }
         // (old == kNonceExhausted: the item was already counted as finished; a late acceptance
         // below the limit still publishes its signature)
         int got = 0;
-        if (g.t == 0) {
+        if (lane == 0) {
             for (unsigned spin = 0; spin < arg.lock_spins; ++spin) {
                 if (atomicCAS(arg.locks + item, 0u, 1u) == 0u) {
                     got = 1;
@@ -680,19 +705,19 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
             }
             if (!got) atomicOr(&q->error, 1u);
         }
-        got = __shfl_sync(g.gmask, got, lane_off);
+        got = __shfl_sync(0xFFFFFFFFu, got, 0);
         if (!got) return;
         __threadfence();
         unsigned cur = 0;
-        if (g.t == 0) cur = *reinterpret_cast<volatile unsigned *>(arg.best + item);
-        cur = __shfl_sync(g.gmask, cur, lane_off);
+        if (lane == 0) cur = *reinterpret_cast<volatile unsigned *>(arg.best + item);
+        cur = __shfl_sync(0xFFFFFFFFu, cur, 0);
         if (cur == nonce) {
-            publish_signature<PM::SIG_BYTES, 16>(arg.sig_out + (size_t)item * arg.sig_pitch,
-                                                 reinterpret_cast<const uint32_t *>(slot + C::SL_SIG), g.t);
+            publish_signature<PM::SIG_BYTES, 32>(arg.sig_out + (size_t)item * arg.sig_pitch,
+                                                 reinterpret_cast<const uint32_t *>(slot + C::SL_SIG), lane);
         }
         __threadfence();
-        __syncwarp(g.gmask);
-        if (g.t == 0) atomicExch(arg.locks + item, 0u);
+        __syncwarp();
+        if (lane == 0) atomicExch(arg.locks + item, 0u);
     };
 
     // w = invNTT(A_hat * NTT(y)), Decompose, pack w1 of one attempt (group-collective)
@@ -762,25 +787,24 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
         __syncwarp(g.gmask);
     };
 
-    // ---------------- NTT phase: rejection of batch cb (jobs < na_c), w = A y of batch nb
+    // ---------------- NTT phase: rejection of batch cb, w = A y of batch nb
     auto ntt_phase = [&](int cb, int na_c, int nb, int na_n) {
-        // w jobs start at an even index, so the two groups of a warp never run a rejection and a w
-        // job side by side (divergent: the warp would run one after the other)
-        const int rpad = (na_c + 1) & ~1;
-        const int total = rpad + na_n;
-        // a warp takes two consecutive jobs, one per 16-thread group, so both groups of the warp
-        // usually run the same job type in lockstep
+        // a warp takes one unit at a time: a rejection unit is one attempt for the whole warp, a w
+        // unit two attempts, one per 16-thread group (w jobs have no data-dependent control flow,
+        // so the two groups run in lockstep)
+        const int total = na_c + (na_n + 1) / 2;
 #pragma unroll 1
         for (;;) {
             unsigned base = 0;
-            if (lane == 0) base = atomicAdd(&s_ctl[CT_NJOB], 2u);
+            if (lane == 0) base = atomicAdd(&s_ctl[CT_NJOB], 1u);
             base = __shfl_sync(0xFFFFFFFFu, base, 0);
             if ((int)base >= total) break;
-            const int job = (int)base + (lane_off ? 1 : 0);
-            if (job < na_c)
-                reject_job(cb, job);
-            else if (job >= rpad && job < total)
-                w_job(nb, job - rpad);
+            if ((int)base < na_c) {
+                reject_job(cb, (int)base);
+            } else {
+                const int a = 2 * ((int)base - na_c) + (lane_off ? 1 : 0);
+                if (a < na_n) w_job(nb, a);
+            }
             __syncwarp();  // both groups back together before the next full-warp grab
         }
     };
