@@ -419,8 +419,54 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
             // the two batches in flight hold different items and no attempt is speculative.
             const unsigned cap = (D == 1u) ? ((pend + 1u) / 2u < (unsigned)A ? (pend + 1u) / 2u : (unsigned)A) : (unsigned)A;
             unsigned filled = 0;
+            // An item with f attempts in flight gets D - f more (none when f >= D).  When all of
+            // them fit the batch (D * pend <= cap), one scan hands each item its attempts with one
+            // atomic on its nonce counter; otherwise pass p gives one more attempt to the items
+            // with at most p in flight, so a full batch spreads its slots over the items.
+            const bool one_scan = D >= 2u && D * pend <= cap;
+            auto place = [&](unsigned pos, unsigned i, unsigned nn) {
+                s_item[buf * A + pos] = i;
+                if (nn < arg.nonce_limit) {
+                    s_nonce[buf * A + pos] = nn;
+                } else {
+                    // every nonce used without acceptance (never for honest keys at the default
+                    // limit): the slot becomes a no-op, and the first lane to get here marks the
+                    // item finished so that the block can exit
+                    s_nonce[buf * A + pos] = 0xFFFFFFFFu;
+                    if (atomicCAS(arg.best + i, 0xFFFFFFFFu, kNonceExhausted) == 0xFFFFFFFFu) {
+                        atomicOr(&q->error, 2u);
+                        atomicSub(&s_ctl[CT_PEND], 1u);
+                    }
+                }
+            };
 #pragma unroll 1
-            for (unsigned pass = 0; pass < D && filled < cap; ++pass) {
+            for (unsigned k0 = 0; one_scan && k0 < n_own; k0 += 32) {
+                const unsigned k = k0 + lane, i = b0 + k * grid;
+                unsigned want = 0;
+                if (k < n_own) {
+                    const unsigned bi = __ldcg(arg.best + i), fi = __ldcg(arg.inflight + i);
+                    want = (bi == 0xFFFFFFFFu && fi < D) ? D - fi : 0u;
+                }
+                unsigned incl = want;  // inclusive prefix sum over the warp
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const unsigned pos0 = filled + incl - want;
+                // (D * pend <= cap keeps every position below cap; the clamp only guards the bound)
+                const unsigned take = pos0 >= cap ? 0u : (want < cap - pos0 ? want : cap - pos0);
+                if (take) {
+                    const unsigned nn = atomicAdd(arg.next_nonce + i, take);
+                    atomicAdd(arg.inflight + i, take);
+#pragma unroll 1
+                    for (unsigned r = 0; r < take; ++r) place(pos0 + r, i, nn + r);
+                }
+                filled += __shfl_sync(0xFFFFFFFFu, incl, 31);
+                if (filled > cap) filled = cap;
+            }
+#pragma unroll 1
+            for (unsigned pass = 0; !one_scan && pass < D && filled < cap; ++pass) {
 #pragma unroll 1
                 for (unsigned k0 = 0; k0 < n_own && filled < cap; k0 += 32) {
                     const unsigned k = k0 + lane, i = b0 + k * grid;
@@ -435,19 +481,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_sign(FusedSign
                     if (ok && pos < cap) {
                         const unsigned nn = atomicAdd(arg.next_nonce + i, 1u);
                         atomicAdd(arg.inflight + i, 1u);
-                        s_item[buf * A + pos] = i;
-                        if (nn < arg.nonce_limit) {
-                            s_nonce[buf * A + pos] = nn;
-                        } else {
-                            // every nonce used without acceptance (never for honest keys at the
-                            // default limit): the slot becomes a no-op, and the first lane to get
-                            // here marks the item finished so that the block can exit
-                            s_nonce[buf * A + pos] = 0xFFFFFFFFu;
-                            if (atomicCAS(arg.best + i, 0xFFFFFFFFu, kNonceExhausted) == 0xFFFFFFFFu) {
-                                atomicOr(&q->error, 2u);
-                                atomicSub(&s_ctl[CT_PEND], 1u);
-                            }
-                        }
+                        place(pos, i, nn);
                     }
                     filled += __popc(bal);
                     if (filled > cap) filled = cap;
