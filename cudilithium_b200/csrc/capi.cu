@@ -69,29 +69,53 @@ __global__ void __launch_bounds__(kBlock) k_derive_rhoprime(uint8_t *out, size_t
 // out = invNTT(NTT(a) o b) for npolys polynomial pairs.  A grid of a few blocks per SM walks the
 // batch: each 16-thread group takes every total_groups-th polynomial, and while it transforms one it
 // already has the loads of the next a (issued before the inverse transform) and of the current b
-// (issued before the forward transform) in flight, so HBM latency overlaps the arithmetic.
+// (issued before the forward transform) in flight, so HBM latency overlaps the arithmetic.  The
+// group positions' register-local twiddles come from a shared-memory copy of the table, read with
+// eight 128-bit loads per transform: holding both directions' rows in registers across the loop
+// would take 64 registers.
 __global__ void __launch_bounds__(kBlock) k_ntt_mul(const int32_t *a, const int32_t *b, int32_t *out, long long npolys) {
     __shared__ int32_t sm[kGroupsPerBlock * NTT_SMEM_WORDS];
+    // twiddle rows (forward, inverse) of the 16 group positions; chunk c (16 bytes) of row t is
+    // stored at chunk (c + t) mod 8, so that the positions' reads of one chunk spread over the banks
+    __shared__ __align__(16) int4 s_tw[2][16][8];
+    for (int k = threadIdx.x; k < 2 * 16 * 8; k += blockDim.x) {
+        const int dir = k >> 7, t = (k >> 3) & 15, c = k & 7;
+        const int4 *src = reinterpret_cast<const int4 *>(dir ? g_group_tw.inv[t] : g_group_tw.fwd[t]);
+        s_tw[dir][t][(c + t) & 7] = src[c];
+    }
+    __syncthreads();
     const long long groups = (long long)gridDim.x * (blockDim.x >> 4);
     long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
     if (p >= npolys) return;
     Group g = make_group(sm, threadIdx.x >> 4);
-    // the thread's twiddles depend only on its group position: loaded once for every polynomial
-    int2 twf[16], twi[16];
-    load_tw16(twf, g_group_tw.fwd[g.t]);
-    load_tw16(twi, g_group_tw.inv[g.t]);
+    auto tw_row = [&](int dir, int2 (&tw)[16]) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int4 v = s_tw[dir][g.t][(c + g.t) & 7];
+            tw[2 * c] = make_int2(v.x, v.y);
+            tw[2 * c + 1] = make_int2(v.z, v.w);
+        }
+    };
     int32_t x[16], y[16];
     load16_strided(x, a + p * N, g.t);
 #pragma unroll 1
     for (; p < npolys; p += groups) {
         load16_contig(y, b + p * N + 16 * g.t);
-        ntt16_tw<false>(x, g.sm, g.gmask, g.t, twf);
+        {
+            int2 tw[16];
+            tw_row(0, tw);
+            ntt16_tw<false>(x, g.sm, g.gmask, g.t, tw);
+        }
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = montmul(x[m], y[m]);
         const long long nx = p + groups;
         int32_t xn[16];
         if (nx < npolys) load16_strided(xn, a + nx * N, g.t);
-        intt16_tw<false>(x, g.sm, g.gmask, g.t, twi);
+        {
+            int2 tw[16];
+            tw_row(1, tw);
+            intt16_tw<false>(x, g.sm, g.gmask, g.t, tw);
+        }
         store16_strided(out + p * N, x, g.t);
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = xn[m];

@@ -105,7 +105,7 @@ struct Impl {
         CUDIL_CK_LAUNCH();
         CUDIL_LAUNCH(KID_SIGN_CHALLENGE, st, k_sign_challenge<MODE><<<blocks_for((size_t)nexec, kItemBlock), kItemBlock, 0, st>>>(pool, sp, tpool, tp, d_exec, nexec, nitems));
         CUDIL_CK_LAUNCH();
-        CUDIL_LAUNCH(KID_SIGN_REJECT, st, k_sign_reject<MODE><<<blocks_for((size_t)nexec * 16), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, d_done, nexec, nitems));
+        CUDIL_LAUNCH(KID_SIGN_REJECT, st, k_sign_reject<MODE><<<blocks_for((size_t)nexec * 32), kBlock, 0, st>>>(pool, sp, mlen, tpool, tp, d_exec, d_done, nexec, nitems));
         CUDIL_CK_LAUNCH();
         return CUDIL_OK;
     }

@@ -299,9 +299,11 @@ __global__ void __launch_bounds__(TB) k_sign_challenge(const uint8_t *sign_pool,
         mo[k] = make_uint4(mask[(4 * k) * TB], mask[(4 * k + 1) * TB], mask[(4 * k + 2) * TB], mask[(4 * k + 3) * TB]);
 }
 
-// One group per attempt: c_hat = NTT(c); z = y + c*s1 (norm check, pack); r0 = w0 - c*s2 and c*t0
-// (norm checks); MakeHint (at most OMEGA, positions in ascending order).  On acceptance the temp
-// row holds the complete signature and done[e] = 1 (src/sign.cu:1010-1195).
+// One warp per attempt: c_hat = NTT(c); r0 = w0 - c*s2, z = y + c*s1 and c*t0 (norm checks);
+// MakeHint (at most OMEGA, positions in ascending order).  The two 16-thread groups of the warp
+// take the attempt's polynomials in pairs (poly 2p + half), so they follow the same control flow
+// and a rejection ends the attempt for the whole warp.  On acceptance the temp row holds the
+// complete signature and done[e] = 1 (src/sign.cu:1010-1195).
 template <int MODE>
 __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_pool, size_t sp, size_t mlen, uint8_t *temp_pool,
                                                         size_t tp, const uint32_t *exec_lut, uint8_t *done, int nexec,
@@ -310,9 +312,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
     using LY = Layout<MODE>;
     constexpr int K = PM::K, L = PM::L, OMEGA = PM::OMEGA;
     __shared__ int32_t sm[kGroupsPerBlock * NTT_SMEM_WORDS];
-    const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 4;
-    if (e >= nexec) return;
+    const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (e >= nexec) return;  // (the same for the whole warp)
     Group g = make_group(sm, threadIdx.x >> 4);
+    const int lane = threadIdx.x & 31, lane_off = lane & 16, half = lane_off >> 4;
     const uint32_t item = exec_lut[e] >> 16;
     if (!bc_ok(item < (uint32_t)nitems, BC_STAGE_ITEM)) return;
     const uint8_t *srow = sign_pool + (size_t)item * sp;
@@ -330,63 +333,71 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
             masks[4 * k + 3] = v.w;
         }
     }
+    // both groups transform c (same data, same instructions)
     int32_t ch[16];
     challenge_strided(ch, masks, g.t);
     ntt16s(ch, g.sm, g.gmask, g.t);
 
     // Acceptance needs every check to pass (src/sign.cu:1026-1144 checks z, then r0, then ct0);
-    // here the most selective runs first: steps r0_0..r0_{K-1} (r0 replaces w0 in the temp row,
-    // for the hints), z_0..z_{L-1}, then ct0_0..ct0_{K-1} with the hints.  One inverse-NTT call
-    // site; the next step's operand loads while the current one transforms.
+    // here the most selective runs first: pair steps of the r0_i (r0 replaces w0 in the temp row,
+    // for the hints), then of the z_j, then of the ct0_i with the hints.  K is even for every
+    // parameter set; L is odd for two of them, so the last z pair may leave the second group
+    // without a polynomial (it transforms zeros and stores nothing).  One inverse-NTT call site;
+    // the next step's key rows load while the current one transforms.
     const int32_t *s1 = reinterpret_cast<const int32_t *>(srow + LY::sg_s1(mlen));
     const int32_t *s2 = reinterpret_cast<const int32_t *>(srow + LY::sg_s2(mlen));
     const int32_t *t0 = reinterpret_cast<const int32_t *>(srow + LY::sg_t0(mlen));
+    constexpr int PR = K / 2, PZ = (L + 1) / 2, NSTEP = 2 * PR + PZ;
     auto operand = [&](int step) -> const int32_t * {
-        if (step < K) return s2 + (size_t)step * N;
-        if (step < K + L) return s1 + (size_t)(step - K) * N;
-        return t0 + (size_t)(step - K - L) * N;
+        if (step < PR) return s2 + (size_t)(2 * step + half) * N;
+        if (step < PR + PZ) {
+            const int j = 2 * (step - PR) + half;
+            return s1 + (size_t)(j < L ? j : L - 1) * N;
+        }
+        return t0 + (size_t)(2 * (step - PR - PZ) + half) * N;
     };
     uint8_t *hs = trow + LY::TP_SIG + PM::SIG_H;
-    const int lane_off = threadIdx.x & 16;
     int cnt = 0;
     int32_t nx[16];
     load16_contig(nx, operand(0) + 16 * g.t);
 #pragma unroll 1
-    for (int step = 0; step < L + 2 * K; ++step) {
-        const bool is_r0 = step < K, is_z = !is_r0 && step < K + L;
-        const int i = is_r0 ? step : step - K - L;
+    for (int step = 0; step < NSTEP; ++step) {
+        const bool is_r0 = step < PR, is_z = !is_r0 && step < PR + PZ;
+        const int k = 2 * (is_r0 ? step : (is_z ? step - PR : step - PR - PZ)) + half;  // i, or j for z
+        const bool act = !is_z || k < L;
         int32_t x[16];
 #pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = montmul(ch[m], nx[m]);
-        if (step + 1 < L + 2 * K) load16_contig(nx, operand(step + 1) + 16 * g.t);
+        for (int m = 0; m < 16; ++m) x[m] = act ? montmul(ch[m], nx[m]) : 0;
+        if (step + 1 < NSTEP) load16_contig(nx, operand(step + 1) + 16 * g.t);
         intt16s(x, g.sm, g.gmask, g.t);
         bool bad = false;
         if (is_z) {
-            const int j = step - K;
             int32_t y[16];
-            unpack_z_strided<MODE>(y, trow + LY::TP_Y + (size_t)j * PM::POLYZ_PACKED, g.t);
+            unpack_z_strided<MODE>(y, trow + LY::TP_Y + (size_t)(act ? k : 0) * PM::POLYZ_PACKED, g.t);
 #pragma unroll
             for (int m = 0; m < 16; ++m) {
-                x[m] = reduce32(x[m] + y[m]);
-                bad |= exceeds(x[m], PM::GAMMA1 - PM::BETA);
+                x[m] = reduce32(x[m] + (act ? y[m] : 0));
+                bad |= act && exceeds(x[m], PM::GAMMA1 - PM::BETA);
             }
-            if (group_any(g, bad)) return;
+            if (__ballot_sync(0xFFFFFFFFu, bad)) return;
             int32_t zc[16];
             strided_to_contig(g, x, zc);
-            uint32_t v[16];
+            if (act) {
+                uint32_t v[16];
 #pragma unroll
-            for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
-            pack16_words<PM::Z_BITS>(
-                reinterpret_cast<uint32_t *>(trow + LY::TP_SIG + PM::SIG_Z + (size_t)j * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
+                for (int m = 0; m < 16; ++m) v[m] = (uint32_t)(PM::GAMMA1 - zc[m]);
+                pack16_words<PM::Z_BITS>(
+                    reinterpret_cast<uint32_t *>(trow + LY::TP_SIG + PM::SIG_Z + (size_t)k * PM::POLYZ_PACKED + g.t * 2 * PM::Z_BITS), v);
+            }
         } else if (is_r0) {
-            int32_t *w0 = reinterpret_cast<int32_t *>(trow + LY::TP_W0) + (size_t)i * N;
+            int32_t *w0 = reinterpret_cast<int32_t *>(trow + LY::TP_W0) + (size_t)k * N;
             int32_t r0[16];
 #pragma unroll
             for (int m = 0; m < 16; ++m) {
                 r0[m] = reduce32(w0[g.t + 16 * m] - x[m]);
                 bad |= exceeds(r0[m], PM::GAMMA2 - PM::BETA);
             }
-            if (group_any(g, bad)) return;
+            if (__ballot_sync(0xFFFFFFFFu, bad)) return;
 #pragma unroll
             for (int m = 0; m < 16; ++m) w0[g.t + 16 * m] = r0[m];
         } else {
@@ -395,26 +406,37 @@ __global__ void __launch_bounds__(kBlock, 4) k_sign_reject(const uint8_t *sign_p
                 x[m] = reduce32(x[m]);
                 bad |= exceeds(x[m], PM::GAMMA2);
             }
-            if (group_any(g, bad)) return;
-            const int32_t *r0 = reinterpret_cast<const int32_t *>(trow + LY::TP_W0) + (size_t)i * N;
-            const uint8_t *w1p = trow + LY::TP_W1P + (size_t)i * PM::POLYW1_PACKED;
+            if (__ballot_sync(0xFFFFFFFFu, bad)) return;
+            const int32_t *r0 = reinterpret_cast<const int32_t *>(trow + LY::TP_W0) + (size_t)k * N;
+            const uint8_t *w1p = trow + LY::TP_W1P + (size_t)k * PM::POLYW1_PACKED;
+            // hint bits of poly k: bit m of hb = hint of coefficient t + 16 m
+            unsigned hb = 0;
 #pragma unroll
             for (int m = 0; m < 16; ++m) {
                 const int32_t w1 = (int32_t)get_bits(w1p, (g.t + 16 * m) * PM::W1_BITS, PM::W1_BITS);
-                const unsigned h = make_hint<MODE>(r0[g.t + 16 * m] + x[m], w1);
-                const unsigned bal = (__ballot_sync(g.gmask, h) >> lane_off) & 0xFFFFu;
-                if (h) {
-                    const int idx = cnt + __popc(bal & ((1u << g.t) - 1u));
-                    if (idx < OMEGA) hs[idx] = (uint8_t)(g.t + 16 * m);
-                }
-                cnt += __popc(bal);
+                hb |= make_hint<MODE>(r0[g.t + 16 * m] + x[m], w1) << m;
             }
-            if (cnt > OMEGA) return;
-            if (g.t == 0) hs[OMEGA + i] = (uint8_t)cnt;
+            // hint counts of both polynomials of the pair, then the positions in ascending
+            // coefficient order: poly 2p first, then poly 2p + 1
+            int tot = __popc(hb);
+#pragma unroll
+            for (int o = 8; o >= 1; o >>= 1) tot += __shfl_xor_sync(0xFFFFFFFFu, tot, o);
+            const int tot0 = __shfl_sync(0xFFFFFFFFu, tot, 0), tot1 = __shfl_sync(0xFFFFFFFFu, tot, 16);
+            if (cnt + tot0 + tot1 > OMEGA) return;
+            int idx = cnt + (half ? tot0 : 0);
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                const unsigned bit = (hb >> m) & 1u;
+                const unsigned bal = (__ballot_sync(0xFFFFFFFFu, bit) >> lane_off) & 0xFFFFu;
+                if (bit) hs[idx + __popc(bal & ((1u << g.t) - 1u))] = (uint8_t)(g.t + 16 * m);
+                idx += __popc(bal);
+            }
+            if (g.t == 0) hs[OMEGA + k] = (uint8_t)(cnt + (half ? tot0 + tot1 : tot0));
+            cnt += tot0 + tot1;
         }
     }
-    for (int q = cnt + g.t; q < OMEGA; q += 16) hs[q] = 0;
-    if (g.t == 0) done[e] = 1;
+    for (int q = cnt + lane; q < OMEGA; q += 32) hs[q] = 0;
+    if (lane == 0) done[e] = 1;
 }
 
 struct CopyEntry {
