@@ -1042,13 +1042,23 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
                     int32_t acc[16];
 #pragma unroll
                     for (int m = 0; m < 16; ++m) acc[m] = 0;
+                    // A row entries in chunks of up to four polynomials: their loads are all in
+                    // flight before the first one is consumed (one memory round trip per chunk)
 #pragma unroll 1
-                    for (int j = 0; j < L; ++j) {
-                        int32_t av[16], zv[16];
-                        load16_contig(av, mat + (size_t)j * N + 16 * g.t);
-                        load16_smem(zv, zh + j * N, g.t);
+                    for (int j0 = 0; j0 < L; j0 += 4) {
+                        int32_t av[4][16];
 #pragma unroll
-                        for (int m = 0; m < 16; ++m) acc[m] += montmul(av[m], zv[m]);
+                        for (int jj = 0; jj < 4; ++jj)
+                            if (j0 + jj < L) load16_contig(av[jj], mat + (size_t)(j0 + jj) * N + 16 * g.t);
+#pragma unroll
+                        for (int jj = 0; jj < 4; ++jj) {
+                            if (j0 + jj < L) {
+                                int32_t zv[16];
+                                load16_smem(zv, zh + (j0 + jj) * N, g.t);
+#pragma unroll
+                                for (int m = 0; m < 16; ++m) acc[m] += montmul(av[jj][m], zv[m]);
+                            }
+                        }
                     }
                     int32_t cv[16], tv[16];
                     load16_smem(cv, zh + L * N, g.t);
