@@ -1042,29 +1042,45 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_fused_verify(const u
                     int32_t acc[16];
 #pragma unroll
                     for (int m = 0; m < 16; ++m) acc[m] = 0;
-                    // A row entries in chunks of up to four polynomials: their loads are all in
-                    // flight before the first one is consumed (one memory round trip per chunk)
+                    // sum_j A_ij z_j - c t1_i, the key operands in chunks of up to four polynomials
+                    // whose loads are all in flight before the first one is consumed (one memory
+                    // round trip per chunk).  When L is not a multiple of four, t1_i joins the last
+                    // chunk of A row entries as operand L (its shared-memory vector, after
+                    // z_hat_0..L-1, is c_hat); otherwise it would start a chunk of its own, and
+                    // the separate load below measured faster.  The int32 sum is exact
+                    // (|acc| < (L+1) q), so both forms give the same result.
+                    const int32_t *t1 = reinterpret_cast<const int32_t *>(row + C::PK_T1) + (size_t)i * N;
+                    constexpr int LAST = (L % 4 == 0) ? L - 1 : L;  // last operand in the chunks
 #pragma unroll 1
-                    for (int j0 = 0; j0 < L; j0 += 4) {
+                    for (int j0 = 0; j0 <= LAST; j0 += 4) {
                         int32_t av[4][16];
 #pragma unroll
                         for (int jj = 0; jj < 4; ++jj)
-                            if (j0 + jj < L) load16_contig(av[jj], mat + (size_t)(j0 + jj) * N + 16 * g.t);
+                            if (j0 + jj <= LAST) load16_contig(av[jj], (j0 + jj < L ? mat + (size_t)(j0 + jj) * N : t1) + 16 * g.t);
 #pragma unroll
                         for (int jj = 0; jj < 4; ++jj) {
-                            if (j0 + jj < L) {
+                            if (j0 + jj <= LAST) {
                                 int32_t zv[16];
                                 load16_smem(zv, zh + (j0 + jj) * N, g.t);
+                                if (j0 + jj < L) {
 #pragma unroll
-                                for (int m = 0; m < 16; ++m) acc[m] += montmul(av[jj][m], zv[m]);
+                                    for (int m = 0; m < 16; ++m) acc[m] += montmul(av[jj][m], zv[m]);
+                                } else {
+#pragma unroll
+                                    for (int m = 0; m < 16; ++m) acc[m] -= montmul(zv[m], av[jj][m]);
+                                }
                             }
                         }
                     }
-                    int32_t cv[16], tv[16];
-                    load16_smem(cv, zh + L * N, g.t);
-                    load16_contig(tv, reinterpret_cast<const int32_t *>(row + C::PK_T1) + (size_t)i * N + 16 * g.t);
+                    if constexpr (LAST < L) {
+                        int32_t cv[16], tv[16];
+                        load16_smem(cv, zh + L * N, g.t);
+                        load16_contig(tv, t1 + 16 * g.t);
 #pragma unroll
-                    for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m] - montmul(cv[m], tv[m]));
+                        for (int m = 0; m < 16; ++m) acc[m] -= montmul(cv[m], tv[m]);
+                    }
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) acc[m] = reduce32(acc[m]);
                     intt16s(acc, g.sm, g.gmask, g.t);
                     int32_t w1[16];
 #pragma unroll
