@@ -5,16 +5,19 @@
 //      secret rows  [rho | K | tr | pad..256 | A_hat (K*L polys) | s1_hat | s2_hat | t0_hat]
 //      public rows  [rho | tr | pad..256 | A_hat (K*L polys) | t1_hat = NTT(t1 * 2^d)]
 //  * k_fused_prehash  one thread per message, longest messages first: mu = H(tr||m), rho' = H(K||mu)
-//  * k_fused_sign     ONE persistent kernel for all signing attempts of a batch.  A device ticket
-//                     queue hands out (item, nonce) attempts -- ticket t is (t mod n, t div n), so the
-//                     nonces of every item are issued in increasing order -- and skips attempts whose
-//                     item already has an accepted smaller nonce.  Each block claims up to A live
-//                     attempts, runs ExpandMask (thread per attempt), w = A*y (16-thread group per
-//                     attempt), challenge (thread per attempt), rejection checks + hints (group per
-//                     attempt) and refills its slots from the queue.  An accepted attempt lowers the
-//                     item's best nonce with atomicMin and, under a per-item lock with a bounded spin,
-//                     publishes its signature only if it still holds the minimum -- the same
-//                     smallest-accepted-nonce result as deterministic signing (src/api.cu:388-411).
+//  * k_fused_sign     ONE persistent kernel for all signing attempts of a batch.  Block b owns the
+//                     items b, b + grid, ...; every item has a next-nonce counter, so its nonces are
+//                     issued in increasing order, and attempts whose item already has an accepted
+//                     smaller nonce are skipped.  Each block claims up to A attempts of its pending
+//                     items at a time (speculating more deeply as they run out) and runs them in two
+//                     phases per iteration: a Keccak phase (ExpandMask, thread per (attempt, j)
+//                     stream; the challenge, thread per attempt) and an NTT phase (w = A*y, 16-thread
+//                     group per attempt; rejection checks + hints, warp per attempt).  An accepted
+//                     attempt lowers the item's best nonce with atomicMin and, under a per-item lock
+//                     with a bounded spin, publishes its signature only if it still holds the
+//                     minimum -- the same smallest-accepted-nonce result as deterministic signing
+//                     (src/api.cu:388-411).  k_fused_sign_async (fused_sign_async.cuh) runs the same
+//                     queue without block-wide phases.
 //  * k_fused_verify   persistent verification against public rows (no ExpandA / H(pk) per signature).
 #pragma once
 
