@@ -231,3 +231,37 @@ def test_engine_long_messages_match_oracle(cuda_ok, oracle, mode, variant):
     assert np.all(eng.verify_np(sig, msgs, key_idx) == 0)
     bad = [m[:-1] + bytes([m[-1] ^ 1]) if m else b"x" for m in msgs]
     assert np.all(eng.verify_np(sig, bad, key_idx) == -1)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_sign_pipeline_batches_match_oracle(cuda_ok, oracle, mode):
+    """SignPipeline: five batches of different messages over two engines on two streams (each
+    batch rebuilds its engine's key caches), every batch's signatures equal the oracle's."""
+    import torch
+    from cudilithium_b200.engine import SignPipeline, pack_messages
+    rng = np.random.default_rng(400 + mode)
+    nk, n, nb = 6, 40, 5
+    p = oracle.params(mode)
+    pk, sk = oracle.keypair_batch(mode, nk, rand_index=610 + mode)
+    d_sk = torch.from_numpy(sk.reshape(-1)).cuda()
+    pipe = SignPipeline(mode, max_keys=nk, max_items=n, depth=2)
+    batches, outs = [], []
+    try:
+        for b in range(nb):
+            lens = rng.integers(0, 200, n)
+            msgs = rand_msgs(rng, n, lens)
+            key_idx = rng.integers(0, nk, n).astype(np.uint32)
+            d_msgs, offs, mlens = pack_messages(msgs)
+            d_sig = torch.empty(n * p.sig_bytes, dtype=torch.uint8, device="cuda")
+            pipe.sign(d_sig, d_msgs, offs, mlens, key_idx, d_sk=d_sk, after=torch.cuda.current_stream())
+            batches.append((msgs, key_idx, d_msgs))
+            outs.append(d_sig)
+        pipe.join()
+        torch.cuda.synchronize()
+        for (msgs, key_idx, _), d_sig in zip(batches, outs):
+            got = d_sig.cpu().numpy().reshape(n, p.sig_bytes)
+            assert np.array_equal(got, oracle_sign(oracle, mode, sk, key_idx, msgs))
+        for e in pipe.engines:
+            assert e.last_status()[1] == 0
+    finally:
+        pipe.close()
