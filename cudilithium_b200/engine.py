@@ -202,19 +202,20 @@ class Engine:
         return d_ret.cpu().numpy()[:n]
 
 
-class SignPipeline:
-    """Signs a stream of batches over ``depth`` engines, each on its own CUDA stream, batch k on
-    engine k mod depth.
+class EnginePipeline:
+    """Runs a stream of batches over ``depth`` engines, each on its own CUDA stream, batch k on
+    engine k mod depth (signing or verification).
 
-    The persistent signer's blocks finish apart: over the last part of a launch more and more SMs
-    have no signer block left.  With one engine on one stream the next batch's key-cache build and
-    prehash wait for the whole launch; with an engine per stream they start on the SMs freed at its
-    end, and so do the first blocks of the next signer.  Batches are independent (each engine keeps
-    its own caches, queue and attempt slots), so every batch's signatures are the same as signed
-    alone.  The same works from C with one ``cudil_engine`` per stream.
+    The persistent kernels' blocks finish apart: over the last part of a launch more and more SMs
+    have no block left.  With one engine on one stream the next batch's key-cache build and prehash
+    wait for the whole launch; with an engine per stream they start on the SMs freed at its end,
+    and so do the first blocks of the next kernel.  Batches are independent (each engine keeps its
+    own caches, queue and scratch), so every batch's results are the same as run alone.  The same
+    works from C with one ``cudil_engine`` per stream.
 
-    ``sign`` returns the stream on which the batch completes; the caller keeps a batch's input and
-    output buffers alive and unchanged until then (``join`` makes a stream wait for every batch).
+    ``sign`` / ``verify`` return the stream on which the batch completes; the caller keeps a
+    batch's input and output buffers alive and unchanged until then (``join`` makes a stream wait
+    for every batch).
     """
 
     def __init__(self, mode: int, max_keys: int, max_items: int, depth: int = 2, threads: int = 0, spec_slots: int = 0):
@@ -224,11 +225,7 @@ class SignPipeline:
         self.streams = [torch.cuda.Stream() for _ in range(depth)]
         self.k = 0
 
-    def sign(self, d_sig: torch.Tensor, d_msgs: torch.Tensor, offsets, mlens, key_idx, d_sk: torch.Tensor | None = None,
-             after=None):
-        """Signs the next batch.  d_sk: packed secret keys whose cache rows this batch's engine
-        builds first (None: the engine's current rows); after: a stream or event the batch waits
-        for (its inputs are ready there)."""
+    def _next(self, after):
         j = self.k % len(self.engines)
         self.k += 1
         s = self.streams[j]
@@ -236,14 +233,30 @@ class SignPipeline:
             s.wait_event(after)
         elif after is not None:
             s.wait_stream(after)
-        e = self.engines[j]
+        return self.engines[j], s
+
+    def sign(self, d_sig: torch.Tensor, d_msgs: torch.Tensor, offsets, mlens, key_idx, d_sk: torch.Tensor | None = None,
+             after=None):
+        """Signs the next batch.  d_sk: packed secret keys whose cache rows this batch's engine
+        builds first (None: the engine's current rows); after: a stream or event the batch waits
+        for (its inputs are ready there)."""
+        e, s = self._next(after)
         if d_sk is not None:
             e.set_secret_keys(d_sk, stream=s)
         e.sign(d_sig, d_msgs, offsets, mlens, key_idx, stream=s)
         return s
 
+    def verify(self, d_ret: torch.Tensor, d_sig: torch.Tensor, d_msgs: torch.Tensor, offsets, mlens, key_idx,
+               d_pk: torch.Tensor | None = None, after=None):
+        """Verifies the next batch (d_pk: packed public keys whose cache rows are built first)."""
+        e, s = self._next(after)
+        if d_pk is not None:
+            e.set_public_keys(d_pk, stream=s)
+        e.verify(d_ret, d_sig, d_msgs, offsets, mlens, key_idx, stream=s)
+        return s
+
     def join(self, stream=None):
-        """Makes `stream` (default: the current stream) wait for every batch signed so far."""
+        """Makes `stream` (default: the current stream) wait for every batch run so far."""
         stream = stream or torch.cuda.current_stream()
         for s in self.streams:
             stream.wait_stream(s)

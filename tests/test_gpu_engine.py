@@ -235,16 +235,17 @@ def test_engine_long_messages_match_oracle(cuda_ok, oracle, mode, variant):
 
 @pytest.mark.parametrize("mode", MODES)
 def test_sign_pipeline_batches_match_oracle(cuda_ok, oracle, mode):
-    """SignPipeline: five batches of different messages over two engines on two streams (each
-    batch rebuilds its engine's key caches), every batch's signatures equal the oracle's."""
+    """EnginePipeline: five batches of different messages over two engines on two streams (each
+    batch rebuilds its engine's key caches), every batch's signatures equal the oracle's, and the
+    same batches verify through the pipeline (a tampered signature is rejected)."""
     import torch
-    from cudilithium_b200.engine import SignPipeline, pack_messages
+    from cudilithium_b200.engine import EnginePipeline, pack_messages
     rng = np.random.default_rng(400 + mode)
     nk, n, nb = 6, 40, 5
     p = oracle.params(mode)
     pk, sk = oracle.keypair_batch(mode, nk, rand_index=610 + mode)
     d_sk = torch.from_numpy(sk.reshape(-1)).cuda()
-    pipe = SignPipeline(mode, max_keys=nk, max_items=n, depth=2)
+    pipe = EnginePipeline(mode, max_keys=nk, max_items=n, depth=2)
     batches, outs = [], []
     try:
         for b in range(nb):
@@ -254,14 +255,30 @@ def test_sign_pipeline_batches_match_oracle(cuda_ok, oracle, mode):
             d_msgs, offs, mlens = pack_messages(msgs)
             d_sig = torch.empty(n * p.sig_bytes, dtype=torch.uint8, device="cuda")
             pipe.sign(d_sig, d_msgs, offs, mlens, key_idx, d_sk=d_sk, after=torch.cuda.current_stream())
-            batches.append((msgs, key_idx, d_msgs))
+            batches.append((msgs, key_idx, d_msgs, offs, mlens))
             outs.append(d_sig)
         pipe.join()
         torch.cuda.synchronize()
-        for (msgs, key_idx, _), d_sig in zip(batches, outs):
+        for (msgs, key_idx, _, _, _), d_sig in zip(batches, outs):
             got = d_sig.cpu().numpy().reshape(n, p.sig_bytes)
             assert np.array_equal(got, oracle_sign(oracle, mode, sk, key_idx, msgs))
         for e in pipe.engines:
             assert e.last_status()[1] == 0
+        # the same batches verified through the pipeline (public-key caches built per batch), one
+        # signature of the last batch tampered with
+        d_pk = torch.from_numpy(pk.reshape(-1)).cuda()
+        outs[-1][p.sig_bytes * 3 + 50] ^= 1
+        rets = []
+        for (msgs, key_idx, d_msgs, offs, mlens), d_sig in zip(batches, outs):
+            d_ret = torch.empty(n, dtype=torch.int32, device="cuda")
+            pipe.verify(d_ret, d_sig, d_msgs, offs, mlens, key_idx, d_pk=d_pk, after=torch.cuda.current_stream())
+            rets.append(d_ret)
+        pipe.join()
+        torch.cuda.synchronize()
+        for b, d_ret in enumerate(rets):
+            want = np.zeros(n, np.int32)
+            if b == nb - 1:
+                want[3] = -1
+            assert np.array_equal(d_ret.cpu().numpy(), want)
     finally:
         pipe.close()
