@@ -1,5 +1,6 @@
 """Autotuner for the fused engine: picks the signer kernel (phased or asynchronous), the block
-size and the per-block speculation target for each parameter set by timing real signing batches, and caches the result as JSON
+size and the per-block speculation target for each parameter set by timing real signing batches
+(a stream of batches over two engines, as EnginePipeline runs them), and caches the result as JSON
 (``cudilithium_b200/tuned.json``, keyed by GPU name).
 
     python -m cudilithium_b200.autotune [--modes 2 3 5] [--batch 16384]
@@ -28,6 +29,7 @@ SPEC = (16, 32, 64, 128)
 # output worse than the 256-thread phased kernel; callers with large batches select it explicitly.
 ASYNC = ((2, 128), (3, 160))
 ROUNDS = 3
+PIPE_BATCHES = 6
 
 
 def _gpu_name() -> str:
@@ -44,7 +46,7 @@ def tuned(mode: int) -> dict:
         return DEFAULTS[mode]
 
 
-def tune_mode(mode: int, batch: int, reps: int = 3) -> dict:
+def tune_mode(mode: int, batch: int) -> dict:
     import numpy as np
     import torch
 
@@ -66,36 +68,48 @@ def tune_mode(mode: int, batch: int, reps: int = 3) -> dict:
     lens = np.full(batch, 32, np.uint32)
     keys = np.arange(batch, dtype=np.uint32)
     sig = torch.empty(batch * pm.sig_bytes, dtype=torch.uint8, device=dev)
-    # every candidate is timed in ROUNDS interleaved rounds (its median is kept), so that a slow
-    # moment of the GPU does not decide between two settings within a few per cent of each other
+    # Every candidate signs a stream of PIPE_BATCHES batches over two engines on two streams (the
+    # way EnginePipeline runs batches: the next batch starts on the SMs the current signer frees),
+    # and is timed in ROUNDS interleaved rounds (its median is kept), so that a slow moment of the
+    # GPU does not decide between two settings within a few per cent of each other.
     engines = {}
     cands = []
     for t in THREADS:
-        e = Engine(mode, batch, batch, threads=t)
-        e.set_secret_keys(sk, stream=spp)
-        engines[t] = e
+        pair = [Engine(mode, batch, batch, threads=t) for _ in range(2)]
+        for e in pair:
+            e.set_secret_keys(sk, stream=spp)
+        engines[t] = pair
         cands += [(t, 0, s) for s in SPEC] + ([(t, v, s) for v, s in ASYNC] if t == THREADS[-1] else [])
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    sigs = [torch.empty_like(sig) for _ in range(2)]
     times = {c: [] for c in cands}
     ref = None
     for _ in range(ROUNDS):
         for t, kern, s in cands:
-            e = engines[t]
-            e.set_sign_kernel(kern)
-            e.set_spec_slots(s)
-            e.sign(sig, m, offs, lens, keys, stream=spp)
+            pair = engines[t]
+            for e in pair:
+                e.set_sign_kernel(kern)
+                e.set_spec_slots(s)
+            pair[0].sign(sig, m, offs, lens, keys, stream=spp)
             torch.cuda.synchronize()
             if ref is None:
                 ref = sig.clone()
             assert torch.equal(sig, ref), "tuning candidates disagree"
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
-            for _ in range(reps):
-                e.sign(sig, m, offs, lens, keys, stream=spp)
+            for x in streams:
+                x.wait_event(a)
+            for k in range(PIPE_BATCHES):
+                pair[k % 2].sign(sigs[k % 2], m, offs, lens, keys, stream=streams[k % 2])
+            cur = torch.cuda.current_stream()
+            for x in streams:
+                cur.wait_stream(x)
             b.record()
             torch.cuda.synchronize()
-            times[(t, kern, s)].append(a.elapsed_time(b) / reps)
-    for e in engines.values():
-        e.close()
+            times[(t, kern, s)].append(a.elapsed_time(b) / PIPE_BATCHES)
+    for pair in engines.values():
+        for e in pair:
+            e.close()
     results = []
     for (t, kern, s), ts in times.items():
         ms = sorted(ts)[len(ts) // 2]

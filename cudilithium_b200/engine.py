@@ -1,8 +1,9 @@
 """Fused engine: per-key resident caches + one persistent, graph-launched kernel per batch.
 
-Python host side of the ``cudil_engine_*`` C ABI (include/cudilithium.h).  A ``SignEngine`` /
-``VerifyEngine`` wraps one engine of one parameter set on the current CUDA device; messages are
-packed into one device buffer at 8-byte aligned offsets (``pack_messages``).
+Python host side of the ``cudil_engine_*`` C ABI (include/cudilithium.h).  An ``Engine`` wraps one
+engine of one parameter set on the current CUDA device; an ``EnginePipeline`` runs a stream of
+batches over several engines on their own streams.  Messages are packed into one device buffer at
+8-byte aligned offsets (``pack_messages``).
 """
 from __future__ import annotations
 
