@@ -52,8 +52,8 @@ OPS_NTT_FWD = 1024 * 6          # 1024 butterflies: 3 IMAD + 3 IADD
 OPS_NTT_INV = 1024 * 6 + 256 * 4  # + the final multiplication by f
 OPS_PW = 5                        # one Montgomery pointwise product
 # k_fused_sign<2,256> (engine sign-kernel variant 0, the tuned Dilithium2 signer), batch 10000:
-# 0.804778 GB read + 0.490499 GB written per launch (ncu)
-FUSED_SIGN_TRAFFIC_BYTES = 0.804778e9 + 0.490499e9
+# 0.771482 GB read + 0.418236 GB written per launch (ncu)
+FUSED_SIGN_TRAFFIC_BYTES = 0.771482e9 + 0.418236e9
 FUSED_SIGN_TRAFFIC_VARIANT = 0
 
 
