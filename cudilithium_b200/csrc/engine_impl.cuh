@@ -71,6 +71,7 @@ struct EngineBase {
     cudaStream_t g_sign_stream = nullptr, g_verify_stream = nullptr;
     size_t device_bytes = 0;
     bool owns_cache = true;  // false when the key caches belong to another engine (attach_keys)
+    const EngineBase *key_src = nullptr;  // that engine: its key rows are read as they stand at each call
     virtual ~EngineBase() = default;
 };
 
@@ -232,6 +233,7 @@ struct EngineImpl : EngineBase {
             cudaFree(pk_cache);
         }
         owns_cache = false;
+        key_src = src->key_src ? src->key_src : src;  // the engine that owns the caches
         sk_cache = src->sk_cache;
         pk_cache = src->pk_cache;
         n_sk = src->n_sk;
@@ -408,6 +410,7 @@ struct EngineImpl : EngineBase {
              const unsigned *key, size_t n, cudaStream_t st, const uint8_t *d_rhop = nullptr,
              const uint8_t *rho_seed = nullptr, unsigned long long rho_counter = 0) {
         if (n == 0) return CUDIL_OK;
+        if (key_src) n_sk = key_src->n_sk;  // rows the owning engine has built by now
         if (!d_sig || !off || !mlen || !key || n > max_items || n_sk == 0) return CUDIL_ERR_INVALID;
         if (!d_msgs) {
             for (size_t i = 0; i < n; ++i)
@@ -476,6 +479,7 @@ struct EngineImpl : EngineBase {
     int verify(int *d_ret, const uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes, const unsigned long long *off,
                const unsigned *mlen, const unsigned *key, size_t n, cudaStream_t st) {
         if (n == 0) return CUDIL_OK;
+        if (key_src) n_pk = key_src->n_pk;
         if (!d_ret || !d_sig || !off || !mlen || !key || n > max_items || n_pk == 0) return CUDIL_ERR_INVALID;
         if (!d_msgs) {
             for (size_t i = 0; i < n; ++i)

@@ -219,10 +219,16 @@ class EnginePipeline:
     for every batch).
     """
 
-    def __init__(self, mode: int, max_keys: int, max_items: int, depth: int = 2, threads: int = 0, spec_slots: int = 0):
+    def __init__(self, mode: int, max_keys: int, max_items: int, depth: int = 2, threads: int = 0, spec_slots: int = 0,
+                 share_keys: bool = False):
+        """share_keys: the engines after the first read the first engine's key caches (for resident
+        keys: build them once through ``engines[0]``, then sign or verify without d_sk / d_pk)."""
         if depth < 1:
             raise ValueError("depth must be at least 1")
         self.engines = [Engine(mode, max_keys, max_items, threads=threads, spec_slots=spec_slots) for _ in range(depth)]
+        if share_keys:
+            for e in self.engines[1:]:
+                e.attach_keys(self.engines[0])
         self.streams = [torch.cuda.Stream() for _ in range(depth)]
         self.k = 0
 
@@ -263,7 +269,7 @@ class EnginePipeline:
             stream.wait_stream(s)
 
     def close(self):
-        for e in self.engines:
+        for e in reversed(self.engines):  # engines sharing the first one's caches go first
             e.close()
 
 

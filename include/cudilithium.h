@@ -232,7 +232,9 @@ int cudil_engine_set_secret_keys(cudil_engine *e, const uint8_t *d_sk, size_t nk
  * queued behind its own host-to-device copy so the copies of later chunks overlap it. */
 int cudil_engine_update_secret_keys(cudil_engine *e, const uint8_t *d_sk, size_t first, size_t nkeys, void *stream);
 /* Share src's key caches (same parameter set; src must outlive e).  An engine created with
- * max_keys = 0 owns no caches and must attach before signing or verifying. */
+ * max_keys = 0 owns no caches and must attach before signing or verifying.  Each sign or verify
+ * call of e uses the key rows the owning engine has built by then, so keys may be set on the owner
+ * before or after attaching (in stream order with e's work, as for the owner's own calls). */
 int cudil_engine_attach_keys(cudil_engine *e, const cudil_engine *src);
 int cudil_engine_set_public_keys(cudil_engine *e, const uint8_t *d_pk, size_t nkeys, void *stream);
 int cudil_engine_sign(cudil_engine *e, uint8_t *d_sig, const uint8_t *d_msgs, size_t msgs_bytes,

@@ -282,3 +282,32 @@ def test_sign_pipeline_batches_match_oracle(cuda_ok, oracle, mode):
             assert np.array_equal(d_ret.cpu().numpy(), want)
     finally:
         pipe.close()
+
+
+def test_pipeline_shared_keys_match_oracle(cuda_ok, oracle):
+    """EnginePipeline(share_keys=True): the key caches are built once through the first engine and
+    read by the second; four batches over the two engines equal the oracle's signatures."""
+    import torch
+    from cudilithium_b200.engine import EnginePipeline, pack_messages
+    mode, nk, n = 3, 5, 30
+    p = oracle.params(mode)
+    rng = np.random.default_rng(77)
+    pk, sk = oracle.keypair_batch(mode, nk, rand_index=720)
+    pipe = EnginePipeline(mode, max_keys=nk, max_items=n, depth=2, share_keys=True)
+    try:
+        pipe.engines[0].set_secret_keys(torch.from_numpy(sk.reshape(-1)).cuda())
+        batches = []
+        for _ in range(4):
+            msgs = rand_msgs(rng, n, rng.integers(0, 500, n))
+            key_idx = rng.integers(0, nk, n).astype(np.uint32)
+            d_msgs, offs, lens = pack_messages(msgs)
+            d_sig = torch.empty(n * p.sig_bytes, dtype=torch.uint8, device="cuda")
+            pipe.sign(d_sig, d_msgs, offs, lens, key_idx, after=torch.cuda.current_stream())
+            batches.append((msgs, key_idx, d_msgs, d_sig))
+        pipe.join()
+        torch.cuda.synchronize()
+        for msgs, key_idx, _, d_sig in batches:
+            got = d_sig.cpu().numpy().reshape(n, p.sig_bytes)
+            assert np.array_equal(got, oracle_sign(oracle, mode, sk, key_idx, msgs))
+    finally:
+        pipe.close()
