@@ -910,6 +910,25 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank, peak_ops) -> dict:
     r5 = torch.empty(nm, dtype=torch.int32, device=dev)
     fused_ms = gpu_ms(lambda: ev5.verify(r5, s5, m5, offs5, lens5, keys5, stream=spp), 5)
     got = r5.cpu().numpy()
+    # the same batch as a stream over two engines sharing the cached public keys (EnginePipeline)
+    pipe5 = EnginePipeline(5, nk, nm, depth=2, share_keys=True)
+    pipe5.engines[0].set_public_keys(pk5, stream=spp)
+    r5q = [torch.empty_like(r5) for _ in range(2)]
+    for k in range(2):
+        pipe5.verify(r5q[k], s5, m5, offs5, lens5, keys5, after=st)
+    pipe5.join(st)
+    torch.cuda.synchronize()
+    K5 = 6
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(st)
+    for k in range(K5):
+        pipe5.verify(r5q[k % 2], s5, m5, offs5, lens5, keys5, after=q0 if k < 2 else None)
+    pipe5.join(st)
+    q1.record(st)
+    torch.cuda.synchronize()
+    pipe_ms5 = q0.elapsed_time(q1) / K5
+    pipe5_same = all(bool(torch.equal(x, r5)) for x in r5q)
+    pipe5.close()
     # plain path on the same signatures (per-signature ExpandA and H(pk)); keys expanded per row
     pk_rows = pk5.view(nk, p5.pk_bytes)[torch.from_numpy(keys5.astype(np.int64)).to(dev)].reshape(-1).contiguous()
     v_pool, vp = alloc_pool(d5.verify_row_bytes(64), nm)
@@ -928,10 +947,13 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank, peak_ops) -> dict:
     out["d5_verify_65536_cached_keys"] = {
         "verify_per_s_fused": nm / (fused_ms / 1e3), "verify_per_s_plain": nm / (plain_ms / 1e3),
         "fused_over_plain": plain_ms / fused_ms, "rejections_exact": bool(np.array_equal(got != 0, expect_bad)),
+        "pipelined": {"verify_per_s": nm / (pipe_ms5 / 1e3), "ms_per_batch": pipe_ms5, "batches": K5,
+                      "fused_over_plain": plain_ms / pipe_ms5, "same_results": pipe5_same,
+                      "note": "the batch repeated as a stream over two engines sharing the key caches, two streams"},
         "fused_equals_plain": bool(torch.equal(r5, r5p)), "flipped": int(flip.size),
         "roofline": alu_roofline(nm * verify_ops(p5, 64, cached=True), fused_ms, peak_ops,
                                  "fused verifier, cached A_hat / t1_hat / tr"),
-        "bit_exact": bool(np.array_equal(got[samp], o_r5) and torch.equal(r5, r5p)),
+        "bit_exact": bool(np.array_equal(got[samp], o_r5) and torch.equal(r5, r5p) and pipe5_same),
         "cpu_baseline": {"verify_per_s": samp.size / t5, "cores": cores, "kind": "port",
                          "sample": f"{samp.size} of the {nm} signatures (flipped ones included), OpenMP over "
                                    f"{cores} threads"}}
