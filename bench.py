@@ -423,7 +423,7 @@ def run_gpu(args) -> dict | None:
     wall0 = time.perf_counter()
     t0p.record(st)
     for k in range(args.steps):
-        pipe.sign(p_sigs[k % 2], d_m, offs, lens, keys, d_sk=d_sk, after=t0p if k < 2 else None)
+        pipe.sign(p_sigs[k % 2], d_m, offs, lens, keys, d_sk=d_sk, after=t0p if k < 2 else False)
     pipe.join(st)
     t1p.record(st)
     barrier()
@@ -436,7 +436,7 @@ def run_gpu(args) -> dict | None:
     barrier()
     t0v.record(st)
     for k in range(args.steps):
-        pipe.verify(p_rets[k % 2], p_sig, d_m, offs, lens, keys, d_pk=d_pk, after=t0v if k < 2 else None)
+        pipe.verify(p_rets[k % 2], p_sig, d_m, offs, lens, keys, d_pk=d_pk, after=t0v if k < 2 else False)
     pipe.join(st)
     t1v.record(st)
     barrier()
@@ -807,7 +807,7 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank, peak_ops) -> dict:
     q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     q0.record(st)
     for k in range(K3):
-        pipe3.sign(s3q[k % 2], d_msgs, offs3, mlens, keys3, after=q0 if k < 2 else None)
+        pipe3.sign(s3q[k % 2], d_msgs, offs3, mlens, keys3, after=q0 if k < 2 else False)
     pipe3.join(st)
     q1.record(st)
     torch.cuda.synchronize()
@@ -924,7 +924,7 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank, peak_ops) -> dict:
     q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     q0.record(st)
     for k in range(K5):
-        pipe5.verify(r5q[k % 2], s5, m5, offs5, lens5, keys5, after=q0 if k < 2 else None)
+        pipe5.verify(r5q[k % 2], s5, m5, offs5, lens5, keys5, after=q0 if k < 2 else False)
     pipe5.join(st)
     q1.record(st)
     torch.cuda.synchronize()

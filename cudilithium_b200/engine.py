@@ -236,9 +236,11 @@ class EnginePipeline:
         j = self.k % len(self.engines)
         self.k += 1
         s = self.streams[j]
+        if after is None:
+            after = torch.cuda.current_stream()
         if isinstance(after, torch.cuda.Event):
             s.wait_event(after)
-        elif after is not None:
+        elif after is not False:
             s.wait_stream(after)
         return self.engines[j], s
 
@@ -246,7 +248,7 @@ class EnginePipeline:
              after=None):
         """Signs the next batch.  d_sk: packed secret keys whose cache rows this batch's engine
         builds first (None: the engine's current rows); after: a stream or event the batch waits
-        for (its inputs are ready there)."""
+        for, where its inputs are ready (default: the current stream; False: no wait)."""
         e, s = self._next(after)
         if d_sk is not None:
             e.set_secret_keys(d_sk, stream=s)
