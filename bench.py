@@ -27,6 +27,7 @@ CPU Dilithium) on the host cores and prints the same metric.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import math
 import os
@@ -83,14 +84,28 @@ def reduce_max(vals, world: int, device):
 
 # ---------------------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clocks and clock-event reasons while the timed region runs (read-only queries).
+
+    Two records: `nvidia-smi -lms 200` over the whole measurement, and an NVML poll every
+    5 ms whose samples count only inside the windows marked with `window()` (the host-side
+    span from the first timed launch to the synchronize after the last).  The reported median
+    and reasons come from the in-window NVML samples when there are any, else from nvidia-smi.
+    """
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    POLL_S = 0.005
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.lines: list[str] = []
+        self.polled: list[tuple[float, float, int]] = []  # (perf_counter, SM MHz, reason bits)
+        self.windows: list[tuple[float, float]] = []
+        self.nvml = None
+        self.max_mhz = None
+        self.done = threading.Event()
 
     def start(self):
         try:
@@ -100,35 +115,84 @@ class ClockSampler:
             threading.Thread(target=self._read, daemon=True).start()
         except OSError:
             self.proc = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.nvml = (pynvml, h)
+            self.bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                         "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                         "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                         "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            self.poller = threading.Thread(target=self._poll, daemon=True)
+            self.poller.start()
+        except Exception:  # no NVML: the nvidia-smi record stands alone
+            self.nvml = None
+        # the first nvidia-smi line shows the sampler is up before anything is timed
+        t_end = time.perf_counter() + 3.0
+        while self.proc is not None and not self.lines and time.perf_counter() < t_end:
+            time.sleep(0.02)
 
     def _read(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
 
+    def _poll(self):
+        nv, h = self.nvml
+        while not self.done.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                bits = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+            except Exception:
+                break
+            self.polled.append((time.perf_counter(), mhz, bits))
+            time.sleep(self.POLL_S)
+
+    @contextlib.contextmanager
+    def window(self):
+        t0 = time.perf_counter()
+        try:
+            yield
+        finally:
+            self.windows.append((t0, time.perf_counter()))
+
     def stop(self) -> dict:
+        self.done.set()
+        if self.nvml is not None:
+            self.poller.join(timeout=1.0)
+            self.nvml[0].nvmlShutdown()
+        smi_sm, smi_max, smi_reasons = [], None, set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            for ln in self.lines:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    smi_sm.append(float(parts[1]))
+                    smi_max = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(self.NAMES, parts[5:9]):
+                    if v.lower() == "active":
+                        smi_reasons.add(nm)
+        inside = [(mhz, bits) for (t, mhz, bits) in self.polled if any(a <= t <= b for a, b in self.windows)]
+        if inside:
+            reasons = sorted(nm for nm in self.NAMES if any(bits & self.bits[nm] for _, bits in inside))
+            return {"sm_mhz": statistics.median(m for m, _ in inside), "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(inside),
+                    "source": "NVML every 5 ms inside the timed regions",
+                    "nvidia_smi": {"sm_mhz": statistics.median(smi_sm) if smi_sm else None, "samples": len(smi_sm),
+                                   "reasons": sorted(smi_reasons)}}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(smi_sm) if smi_sm else None, "sm_max_mhz": smi_max,
+                "reasons": sorted(smi_reasons), "samples": len(smi_sm), "source": "nvidia-smi -lms 200"}
 
 
 # ---------------------------------------------------------------------------- CPU legs
@@ -421,12 +485,13 @@ def run_gpu(args) -> dict | None:
     t0p, t1p = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     wall0 = time.perf_counter()
-    t0p.record(st)
-    for k in range(args.steps):
-        pipe.sign(p_sigs[k % 2], d_m, offs, lens, keys, d_sk=d_sk, after=t0p if k < 2 else False)
-    pipe.join(st)
-    t1p.record(st)
-    barrier()
+    with clocks.window():
+        t0p.record(st)
+        for k in range(args.steps):
+            pipe.sign(p_sigs[k % 2], d_m, offs, lens, keys, d_sk=d_sk, after=t0p if k < 2 else False)
+        pipe.join(st)
+        t1p.record(st)
+        barrier()
     wall = time.perf_counter() - wall0
     launches = lib.cudil_launch_count() - launches0
     # the verification steps, pipelined the same way (public-key caches built per step)
@@ -434,20 +499,22 @@ def run_gpu(args) -> dict | None:
         x.fill_(1)
     t0v, t1v = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
-    t0v.record(st)
-    for k in range(args.steps):
-        pipe.verify(p_rets[k % 2], p_sig, d_m, offs, lens, keys, d_pk=d_pk, after=t0v if k < 2 else False)
-    pipe.join(st)
-    t1v.record(st)
-    barrier()
+    with clocks.window():
+        t0v.record(st)
+        for k in range(args.steps):
+            pipe.verify(p_rets[k % 2], p_sig, d_m, offs, lens, keys, d_pk=d_pk, after=t0v if k < 2 else False)
+        pipe.join(st)
+        t1v.record(st)
+        barrier()
     # the same steps one batch at a time (one engine, one stream each for signing and verification)
     tfs, tfv = Timer(torch, st), Timer(torch, st)
-    for _ in range(args.steps):
-        with tfs:
-            fused_sign()
-        with tfv:
-            fused_verify()
-    barrier()
+    with clocks.window():
+        for _ in range(args.steps):
+            with tfs:
+                fused_sign()
+            with tfv:
+                fused_verify()
+        barrier()
     clk = clocks.stop()
     pipe_ms, pv_ms, fs_ms, fv_ms = max_over_ranks(t0p.elapsed_time(t1p), t0v.elapsed_time(t1v), tfs.total_ms(),
                                                   tfv.total_ms())
