@@ -97,8 +97,9 @@ class ClockSampler:
     NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
     POLL_S = 0.005
 
-    def __init__(self, index: int):
-        self.index = index
+    def __init__(self, index: int, pci_bus_id: str | None = None):
+        self.index = index  # CUDA ordinal; the PCI bus id, when given, picks the same GPU in NVML
+        self.pci_bus_id = pci_bus_id
         self.proc = None
         self.lines: list[str] = []
         self.polled: list[tuple[float, float, int]] = []  # (perf_counter, SM MHz, reason bits)
@@ -108,17 +109,19 @@ class ClockSampler:
         self.done = threading.Event()
 
     def start(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            threading.Thread(target=self._read, daemon=True).start()
-        except OSError:
-            self.proc = None
+        smi_id = self.index
         try:
             import pynvml
             pynvml.nvmlInit()
-            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            h = None
+            if self.pci_bus_id:
+                try:
+                    h = pynvml.nvmlDeviceGetHandleByPciBusId(self.pci_bus_id)
+                except Exception:
+                    h = None
+            if h is None:
+                h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            smi_id = int(pynvml.nvmlDeviceGetIndex(h))
             self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
             self.nvml = (pynvml, h)
             self.bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
@@ -129,6 +132,13 @@ class ClockSampler:
             self.poller.start()
         except Exception:  # no NVML: the nvidia-smi record stands alone
             self.nvml = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={smi_id}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
         # the first nvidia-smi line shows the sampler is up before anything is timed
         t_end = time.perf_counter() + 3.0
         while self.proc is not None and not self.lines and time.perf_counter() < t_end:
@@ -475,7 +485,8 @@ def run_gpu(args) -> dict | None:
     assert all(torch.equal(x, p_sig) for x in p_sigs), "pipelined and plain signatures differ"
     assert int((f_ret != 0).sum().item()) == 0, "fused verify rejected valid signatures"
 
-    clocks = ClockSampler(local)
+    props = torch.cuda.get_device_properties(dev)
+    clocks = ClockSampler(local, "%08x:%02x:%02x.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id))
     clocks.start()
     time.sleep(0.3)
     barrier()
