@@ -792,14 +792,25 @@ def run_configs(args, torch, np, lib, _lib, dev, spp, rank, peak_ops) -> dict:
         lib.cudil_verify_dev(2, pret.data_ptr(), psig.data_ptr(), pm.sig_bytes, pm.sig_bytes, m.data_ptr(), 32, 32,
                              pk.data_ptr(), v_pool.data_ptr(), vp, n, spp)
 
+    # the verifier's public-key cache depends only on the key pairs: it is built on a second stream
+    # while the batch is signed, and verification waits for both
+    s_pk = torch.cuda.Stream(device=dev)
+    e_keys, e_pkc = torch.cuda.Event(), torch.cuda.Event()
+
     def c1_fused():
         lib.cudil_keypair_dev(2, pk.data_ptr(), sk.data_ptr(), None, pool.data_ptr(), kpp, n, spp, 0)
+        e_keys.record(st)
+        s_pk.wait_event(e_keys)
+        ev.set_public_keys(pk, stream=s_pk)
+        e_pkc.record(s_pk)
         es.set_secret_keys(sk, stream=spp)
         es.sign(sig, m, offs, lens, keys, stream=spp)
-        ev.set_public_keys(pk, stream=spp)
+        st.wait_event(e_pkc)
         ev.verify(ret, sig, m, offs, lens, keys, stream=spp)
 
-    res = {"plain_ms": gpu_ms(c1_plain, 5), "fused_ms": gpu_ms(c1_fused, 5)}
+    res = {"plain_ms": gpu_ms(c1_plain, 5), "fused_ms": gpu_ms(c1_fused, 5),
+           "fused_path": "keygen; secret-key cache build and signing, with the public-key cache build on a "
+                         "second stream beside them; verify (fused engines)"}
     res["fused_over_plain"] = res["plain_ms"] / res["fused_ms"]
     alg1, _ = algorithmic_attempts(es.last_nonces(n), *es.last_work())
     ops1 = n * (keygen_ops(pm) + sign_prehash_ops(32) + verify_ops(pm, 32, cached=False)) \
