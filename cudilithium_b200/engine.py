@@ -222,15 +222,23 @@ class EnginePipeline:
     def __init__(self, mode: int, max_keys: int, max_items: int, depth: int = 2, threads: int = 0, spec_slots: int = 0,
                  share_keys: bool = False):
         """share_keys: the engines after the first read the first engine's key caches (for resident
-        keys: build them once through ``engines[0]``, then sign or verify without d_sk / d_pk)."""
+        keys: build them once through ``engines[0]``, then sign or verify without d_sk / d_pk).  The
+        shared rows are read by batches on every stream, so rebuild them through ``engines[0]``
+        only after ``join`` on the stream that builds them."""
         if depth < 1:
             raise ValueError("depth must be at least 1")
         self.engines = [Engine(mode, max_keys, max_items, threads=threads, spec_slots=spec_slots) for _ in range(depth)]
+        self.share_keys = share_keys
         if share_keys:
             for e in self.engines[1:]:
                 e.attach_keys(self.engines[0])
         self.streams = [torch.cuda.Stream() for _ in range(depth)]
         self.k = 0
+
+    def _check_keys_arg(self, d_keys, name: str):
+        if d_keys is not None and self.share_keys:
+            raise ValueError(f"{name} per batch needs engines with caches of their own (share_keys=False); with "
+                             f"shared caches build them once through engines[0]")
 
     def _next(self, after):
         j = self.k % len(self.engines)
@@ -249,6 +257,7 @@ class EnginePipeline:
         """Signs the next batch.  d_sk: packed secret keys whose cache rows this batch's engine
         builds first (None: the engine's current rows); after: a stream or event the batch waits
         for, where its inputs are ready (default: the current stream; False: no wait)."""
+        self._check_keys_arg(d_sk, "d_sk")
         e, s = self._next(after)
         if d_sk is not None:
             e.set_secret_keys(d_sk, stream=s)
@@ -258,6 +267,7 @@ class EnginePipeline:
     def verify(self, d_ret: torch.Tensor, d_sig: torch.Tensor, d_msgs: torch.Tensor, offsets, mlens, key_idx,
                d_pk: torch.Tensor | None = None, after=None):
         """Verifies the next batch (d_pk: packed public keys whose cache rows are built first)."""
+        self._check_keys_arg(d_pk, "d_pk")
         e, s = self._next(after)
         if d_pk is not None:
             e.set_public_keys(d_pk, stream=s)

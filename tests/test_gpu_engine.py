@@ -309,5 +309,12 @@ def test_pipeline_shared_keys_match_oracle(cuda_ok, oracle):
         for msgs, key_idx, _, d_sig in batches:
             got = d_sig.cpu().numpy().reshape(n, p.sig_bytes)
             assert np.array_equal(got, oracle_sign(oracle, mode, sk, key_idx, msgs))
+        # per-batch keys need caches of each engine's own: refused before anything is queued
+        k0 = pipe.k
+        msgs, key_idx, d_msgs, d_sig = batches[0]
+        _, offs, lens = pack_messages(msgs)
+        with pytest.raises(ValueError):
+            pipe.sign(d_sig, d_msgs, offs, lens, key_idx, d_sk=torch.from_numpy(sk.reshape(-1)).cuda())
+        assert pipe.k == k0
     finally:
         pipe.close()
