@@ -318,3 +318,47 @@ def test_pipeline_shared_keys_match_oracle(cuda_ok, oracle):
         assert pipe.k == k0
     finally:
         pipe.close()
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_public_key_cache_built_beside_signing(cuda_ok, oracle, mode):
+    """The verifier's public-key cache is built on a second stream while another engine signs (the
+    keygen + sign + verify sequence); verification on the first stream waits for both.  Signatures
+    equal the oracle's, every one verifies, and a tampered one is rejected."""
+    import torch
+    from cudilithium_b200.engine import Engine, pack_messages
+    rng = np.random.default_rng(140 + mode)
+    nk, n = 6, 64
+    p = oracle.params(mode)
+    pk, sk = oracle.keypair_batch(mode, nk, rand_index=1300 + mode)
+    msgs = rand_msgs(rng, n, rng.integers(0, 300, n))
+    key_idx = rng.integers(0, nk, n).astype(np.uint32)
+    d_msgs, offs, lens = pack_messages(msgs)
+    es, ev = Engine(mode, max_keys=nk, max_items=n), Engine(mode, max_keys=nk, max_items=n)
+    try:
+        st = torch.cuda.current_stream()
+        side = torch.cuda.Stream()
+        d_pk = torch.from_numpy(pk.reshape(-1)).cuda()
+        d_sk = torch.from_numpy(sk.reshape(-1)).cuda()
+        keys_ready, pk_ready = torch.cuda.Event(), torch.cuda.Event()
+        keys_ready.record(st)
+        side.wait_event(keys_ready)
+        ev.set_public_keys(d_pk, stream=side)
+        pk_ready.record(side)
+        d_sig = torch.empty(n * p.sig_bytes, dtype=torch.uint8, device="cuda")
+        es.set_secret_keys(d_sk, stream=st)
+        es.sign(d_sig, d_msgs, offs, lens, key_idx, stream=st)
+        st.wait_event(pk_ready)
+        d_sig[p.sig_bytes * 7] ^= 1  # item 7 tampered after signing, before verification
+        ret = torch.full((n,), 7, dtype=torch.int32, device="cuda")
+        ev.verify(ret, d_sig, d_msgs, offs, lens, key_idx, stream=st)
+        torch.cuda.synchronize()
+        want = oracle_sign(oracle, mode, sk, key_idx, msgs)
+        want[7, 0] ^= 1
+        assert np.array_equal(d_sig.cpu().numpy().reshape(n, p.sig_bytes), want)
+        r = ret.cpu().numpy()
+        assert r[7] == -1
+        assert np.all(np.delete(r, 7) == 0)
+    finally:
+        es.close()
+        ev.close()
